@@ -1,0 +1,356 @@
+"""Benchmark of halloc-b200: 16-byte malloc/free pairs per second.
+
+Workload (the plain-throughput configuration): one kernel of 256 blocks x
+128 threads (32,768 threads) over a 512 MiB pool with default options; each
+thread runs 10 iterations of hamalloc(16), a 16-byte write of
+{tid^0, tid^1, tid^2, tid^3}, a checksummed read-back and hafree.  A step is
+one such launch: 327,680 pairs.  The same loop with CUDA's in-kernel
+malloc/free is timed beside it, and the reference allocator's own code
+(built for the host) is timed on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun as independent replicas (one pool per GPU, no
+collective on the data path; "weak" scaling): value = all pairs / max time.
+Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NTHREADS, BLOCK, NITERS, NALLOCS, NBYTES = 32768, 128, 10, 1, 16
+POOL = 512 << 20
+PAIRS_PER_STEP = NTHREADS * NITERS * NALLOCS
+ATOMICS_PER_PAIR = 2  # one bit-array reservation + one release
+METRIC = "16B malloc/free pairs/s"
+WORKLOAD = ("plain: 256 blocks x 128 threads, hamalloc(16) + 16-B write + read-back + hafree, "
+            "10 iterations per thread, 512 MiB pool, default halloc_opts_t")
+
+
+def plain_checksum(nthreads: int, per_thread: int) -> int:
+    t = np.arange(nthreads, dtype=np.int64)
+    return int(per_thread * (4 * (t - t % 4) + 6).sum())
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ---- clocks during the timed region ---------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9 and f[1].isdigit():
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(int(r[1]) for r in rows),
+                "sm_max_mhz": max(int(r[2]) for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---- our arm ----------------------------------------------------------------
+
+def measure_atomic_peak(torch, H, stream) -> dict:
+    """Distinct-address 32-bit atomic OR throughput over all SMs (the L2
+    atomic roofline denominator), with and without a used return value."""
+    nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    nthreads = nsm * 2048
+    buf = torch.zeros(nthreads, dtype=torch.int32, device="cuda")
+    reps = 256
+    out = {}
+    for returning in (True, False):
+        for _ in range(3):
+            H.atomic_peak(buf, nthreads, nthreads, reps, returning, stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 0.0
+        for _ in range(5):
+            e0.record(stream)
+            H.atomic_peak(buf, nthreads, nthreads, reps, returning, stream)
+            e1.record(stream)
+            e1.synchronize()
+            best = max(best, nthreads * reps / (e0.elapsed_time(e1) * 1e-3))
+        out["returning" if returning else "fire_and_forget"] = best / 1e9
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import halloc_b200 as H
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.current_stream()
+    H.init(H.HallocOpts(memory=POOL))
+    H.l2_persist(stream)
+
+    out = torch.zeros(2, dtype=torch.int64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step():
+        H.throughput(out, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    out.zero_()
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clocks:
+        for e0, e1 in evs:
+            flush.zero_()
+            e0.record(stream)
+            step()
+            e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in evs]
+    total_s = sum(step_ms) * 1e-3
+    cs, nfail = out.cpu().tolist()
+    want = plain_checksum(NTHREADS, NITERS * NALLOCS) * args.steps
+    ok = (nfail == 0 and cs == want and H.status() == 0)
+
+    # end to end through the C ABI from host memory (pinned): H2D of the
+    # per-thread request sizes, kernel, D2H of (checksum, failures)
+    h_sizes = torch.full((NTHREADS,), NBYTES, dtype=torch.int32).pin_memory()
+    d_sizes = torch.empty(NTHREADS, dtype=torch.int32, device="cuda")
+    h_out = torch.zeros(2, dtype=torch.int64).pin_memory()
+    d_out = torch.zeros(2, dtype=torch.int64, device="cuda")
+
+    def e2e_step():
+        H.throughput_host(h_out.data_ptr(), d_out, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS,
+                          h_sizes=h_sizes.data_ptr(), d_sizes=d_sizes, stream=stream)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    e2e_s = 0.0
+    e2e_ok = True
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s += time.perf_counter() - t0
+        e2e_ok &= (int(h_out[1]) == 0 and
+                   int(h_out[0]) == plain_checksum(NTHREADS, NITERS * NALLOCS))
+
+    # max over ranks
+    t = torch.tensor([total_s, e2e_s, 0.0 if ok and e2e_ok else 1.0], dtype=torch.float64,
+                     device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_s, e2e_s, bad = t.tolist()
+
+    res = {"step_ms": step_ms, "total_s": total_s, "e2e_s": e2e_s, "ok": bad == 0.0,
+           "clocks": clocks.summary()}
+    if rank == 0:
+        res["peak"] = measure_atomic_peak(torch, H, stream)
+        # CUDA in-kernel malloc on the same loop
+        cout = torch.zeros(2, dtype=torch.int64, device="cuda")
+        H.cuda_throughput(cout, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS, stream=stream)
+        torch.cuda.synchronize()
+        cout.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        csteps = max(2, min(5, args.steps))
+        ms = 0.0
+        for _ in range(csteps):
+            flush.zero_()
+            e0.record(stream)
+            H.cuda_throughput(cout, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS, stream=stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        cnf = int(cout[1])
+        res["cuda_malloc"] = {"value": PAIRS_PER_STEP * csteps / (ms * 1e-3), "steps": csteps,
+                              "failed_allocs": cnf,
+                              "heap_bytes": H.stats()["cuda_heap_bytes"]}
+    H.shutdown()
+    return res
+
+
+def cpu_sample(kind: str, seconds: float) -> dict:
+    """The plain workload replayed on the host cores; repeats the full
+    workload until about `seconds` have passed."""
+    import oracle
+    cores = os.cpu_count() or 1
+    dt1, _, _ = oracle.cpu_plain_run(kind, NTHREADS, NITERS, NBYTES, cores)
+    reps = max(1, int(seconds / max(dt1, 1e-3)))
+    tot, pairs = 0.0, 0
+    for _ in range(reps):
+        dt, cs, nf = oracle.cpu_plain_run(kind, NTHREADS, NITERS, NBYTES, cores)
+        if nf or cs != plain_checksum(NTHREADS, NITERS):
+            raise RuntimeError(f"CPU {kind} run failed")
+        tot += dt
+        pairs += PAIRS_PER_STEP
+    return {"value": pairs / tot, "unit": "pairs/s", "cores": cores,
+            "sample": f"{reps} runs of the full workload ({PAIRS_PER_STEP} pairs each) on "
+                      f"{cores} host threads"}
+
+
+def reference_kind():
+    import oracle
+    return "reference" if oracle.reference_available() else "port"
+
+
+def main_ours(args):
+    rank, world, local_rank = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        value = PAIRS_PER_STEP * args.steps * world / res["total_s"]
+        e2e = PAIRS_PER_STEP * args.steps * world / res["e2e_s"]
+        peak = max(res["peak"].values()) * 1e9
+        achieved = value / world * ATOMICS_PER_PAIR
+        kind = reference_kind()
+        cpu = cpu_sample(kind, args.cpu_seconds) if world == 1 else None
+        if cpu:
+            cpu["kind"] = kind
+        glibc = cpu_sample("glibc", min(3.0, args.cpu_seconds)) if world == 1 else None
+        line = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["total_s"] * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "threads": NTHREADS, "block": BLOCK,
+                       "iters": NITERS, "block_bytes": NBYTES, "pool_bytes": POOL,
+                       "pairs_per_step": PAIRS_PER_STEP, "parallelism": f"replicas{world}",
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "ok": res["ok"],
+            "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": NTHREADS * 4,
+                    "d2h_bytes_per_step": 16,
+                    "how": "ha_throughput_host_c from pinned host memory, wall clock"},
+            "roofline": {"bound": "l2_atomic", "achieved": achieved / 1e9, "peak": peak / 1e9,
+                         "unit": "Gatomic/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured live: distinct-address u32 atomicOr, "
+                                        f"{res['peak']}",
+                         "algorithmic_atomics_per_pair": ATOMICS_PER_PAIR},
+            "cpu_baseline": cpu,
+            "host_malloc_baseline": glibc,
+            "cuda_malloc_baseline": res.get("cuda_malloc"),
+            "vs_cuda_malloc": value / world / res["cuda_malloc"]["value"]
+            if res.get("cuda_malloc") else None,
+            "gpu_launches": args.steps,
+            "clocks": res["clocks"],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    kind = reference_kind()
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.cpu_plain_run(kind, NTHREADS, NITERS, NBYTES, cores)
+    tot = 0.0
+    for _ in range(args.steps):
+        dt, cs, nf = oracle.cpu_plain_run(kind, NTHREADS, NITERS, NBYTES, cores)
+        if nf or cs != plain_checksum(NTHREADS, NITERS):
+            raise RuntimeError("reference run failed")
+        tot += dt
+    value = PAIRS_PER_STEP * args.steps / tot
+    sample = (f"{args.steps} runs of the full workload ({PAIRS_PER_STEP} pairs each) through "
+              + ("the reference allocator's own code built for the host (oracle/_ref)"
+                 if kind == "reference" else "the host replay model (oracle port)")
+              + f" on {cores} host threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "threads": NTHREADS, "iters": NITERS,
+                   "block_bytes": NBYTES, "pool_bytes": POOL},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = p.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        main_reference(args)
+    else:
+        main_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,273 @@
+"""halloc-b200: host side of the B200 device allocator.
+
+The allocator lives in device code (``hamalloc`` / ``hafree``,
+include/halloc.h).  This module binds the C ABI of ``libhalloc_b200.so``
+(include/halloc_c.h) with ctypes, mirroring the reference's host interface
+(``ha_init(halloc_opts_t)``, ``ha_shutdown``, ``ha_extfrag``) and its test
+harness wrappers (batch malloc / free, the private-throughput loop).
+
+Device buffers are passed as integers (device addresses, e.g.
+``tensor.data_ptr()``) or as objects with a ``data_ptr()`` method; streams
+as integers (``torch.cuda.current_stream().cuda_stream``) or None for the
+default stream.  There is no CPU fallback: every call needs the native
+library and a CUDA device, and raises HallocError otherwise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+__all__ = [
+    "HallocError", "HallocOpts", "init", "shutdown", "extfrag", "stats", "status",
+    "clear_status", "set_wait_limit", "dump_state", "l2_persist", "malloc_batch",
+    "free_batch", "throughput", "throughput_host", "cuda_throughput", "trace",
+    "atomic_peak", "debug_set_head_lock", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
+]
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+SO_PATH = os.path.join(PKG, "libhalloc_b200.so")
+
+HA_OK, HA_EINVAL, HA_ECUDA, HA_ESTATE, HA_ERANGE = 0, -1, -2, -3, -4
+ST_TIMEOUT, ST_BAD_FREE, ST_LIVELOCK = 0x1, 0x2, 0x4
+NSIZES = 16
+NSETS = 37
+NONE = 0xFFFFFFFF
+
+_ERR = {HA_EINVAL: "invalid argument", HA_ECUDA: "CUDA error",
+        HA_ESTATE: "wrong allocator state (not / already initialised)",
+        HA_ERANGE: "size beyond a documented limit"}
+
+
+class HallocError(RuntimeError):
+    pass
+
+
+@dataclass
+class HallocOpts:
+    """Mirror of ``halloc_opts_t`` (include/halloc.h; defaults of halloc
+    src/halloc.h:30-33)."""
+
+    memory: int = 512 << 20
+    halloc_fraction: float = 0.75
+    busy_fraction: float = 0.835
+    roomy_fraction: float = 0.6
+    sparse_fraction: float = 0.012
+    sb_sz_sh: int = 22
+
+
+class _COpts(ctypes.Structure):
+    _fields_ = [("memory", ctypes.c_uint64), ("halloc_fraction", ctypes.c_double),
+                ("busy_fraction", ctypes.c_double), ("roomy_fraction", ctypes.c_double),
+                ("sparse_fraction", ctypes.c_double), ("sb_sz_sh", ctypes.c_int32)]
+
+
+class _CStats(ctypes.Structure):
+    _fields_ = [("pool_base", ctypes.c_uint64), ("pool_bytes", ctypes.c_uint64),
+                ("cuda_heap_bytes", ctypes.c_uint64), ("used_chunks", ctypes.c_uint64),
+                ("used_bytes", ctypes.c_uint64), ("nsbs", ctypes.c_uint32),
+                ("sb_sz", ctypes.c_uint32), ("free_slabs", ctypes.c_uint32),
+                ("head_slabs", ctypes.c_uint32), ("status", ctypes.c_uint32),
+                ("n_head_changes", ctypes.c_uint32), ("n_null", ctypes.c_uint32),
+                ("heap_limit_ok", ctypes.c_uint32), ("head", ctypes.c_uint32 * 16),
+                ("cached", ctypes.c_uint32 * 16)]
+
+
+class _CDump(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in (
+        "tickets", "heads", "cached", "size_infos", "counters", "size_id", "chunk_id",
+        "is_head", "chunk_enc", "sets", "bits", "nibbles")]
+
+
+_vp, _u32, _i64, _int = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int64, ctypes.c_int
+_SIGS = {
+    "ha_init_c": (_int, [ctypes.POINTER(_COpts)]),
+    "ha_shutdown_c": (_int, []),
+    "ha_extfrag_c": (ctypes.c_double, [_int]),
+    "ha_stats_c": (_int, [ctypes.POINTER(_CStats)]),
+    "ha_status_c": (_u32, []),
+    "ha_clear_status_c": (_int, []),
+    "ha_set_wait_limit_c": (_int, [_u32]),
+    "ha_dump_state_c": (_int, [ctypes.POINTER(_CDump)]),
+    "ha_l2_persist_c": (_int, [_vp]),
+    "ha_debug_set_head_lock_c": (_int, [_u32, _u32]),
+    "ha_malloc_batch_c": (_int, [_vp, _u32, _u32, _vp, _int, _vp]),
+    "ha_free_batch_c": (_int, [_vp, _u32, _u32, _vp]),
+    "ha_throughput_c": (_int, [_vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp]),
+    "ha_throughput_host_c": (_int, [_vp, _vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp, _vp]),
+    "ha_cuda_throughput_c": (_int, [_vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp]),
+    "ha_trace_c": (_int, [_vp, _i64, _vp, _vp]),
+    "ha_atomic_peak_c": (_int, [_vp, _u32, _u32, _u32, _int, _vp]),
+}
+
+_lib = None
+
+
+def library_path() -> str:
+    return SO_PATH
+
+
+def load():
+    """Loads libhalloc_b200.so (raises HallocError when it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO_PATH):
+            raise HallocError(f"{SO_PATH} is missing: build it with python -m halloc_b200.build")
+        lib = ctypes.CDLL(SO_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != HA_OK:
+        raise HallocError(f"{what}: {_ERR.get(rc, rc)}")
+
+
+def _addr(x) -> int:
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    raise TypeError(f"cannot take the address of {type(x)}")
+
+
+def _stream(s) -> int:
+    if s is None:
+        return 0
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream
+
+
+# ---- init / shutdown / statistics ------------------------------------------
+
+def init(opts: HallocOpts | None = None) -> None:
+    """ha_init on the current device (error if already initialised)."""
+    o = opts or HallocOpts()
+    c = _COpts(o.memory, o.halloc_fraction, o.busy_fraction, o.roomy_fraction,
+               o.sparse_fraction, o.sb_sz_sh)
+    _check(load().ha_init_c(ctypes.byref(c)), "ha_init_c")
+
+
+def shutdown() -> None:
+    _check(load().ha_shutdown_c(), "ha_shutdown_c")
+
+
+def extfrag(ideal: bool = False) -> float:
+    v = load().ha_extfrag_c(1 if ideal else 0)
+    if v < 0:
+        raise HallocError("ha_extfrag_c failed")
+    return v
+
+
+def stats() -> dict:
+    s = _CStats()
+    _check(load().ha_stats_c(ctypes.byref(s)), "ha_stats_c")
+    d = {f: getattr(s, f) for f, _ in _CStats._fields_ if f not in ("head", "cached")}
+    d["head"] = list(s.head)
+    d["cached"] = list(s.cached)
+    return d
+
+
+def status() -> int:
+    v = load().ha_status_c()
+    if v == 0xFFFFFFFF:
+        raise HallocError("ha_status_c failed")
+    return v
+
+
+def clear_status() -> None:
+    _check(load().ha_clear_status_c(), "ha_clear_status_c")
+
+
+def set_wait_limit(microseconds: int) -> None:
+    _check(load().ha_set_wait_limit_c(microseconds), "ha_set_wait_limit_c")
+
+
+def dump_state() -> dict:
+    """Full device state as numpy arrays (see ha_dump_state_c)."""
+    st = stats()
+    n, sb = st["nsbs"], st["sb_sz"]
+    nw = (n + 31) // 32
+    arrs = {
+        "tickets": np.zeros(NSIZES, np.uint32), "heads": np.zeros(NSIZES, np.uint32),
+        "cached": np.zeros(NSIZES, np.uint32), "size_infos": np.zeros(NSIZES * 8, np.uint32),
+        "counters": np.zeros(n, np.uint32), "size_id": np.zeros(n, np.uint32),
+        "chunk_id": np.zeros(n, np.uint32), "is_head": np.zeros(n, np.uint32),
+        "chunk_enc": np.zeros(n, np.uint32), "sets": np.zeros(NSETS * nw, np.uint32),
+        "bits": np.zeros(n * (sb // 512), np.uint32), "nibbles": np.zeros(n * (sb // 128), np.uint32),
+    }
+    d = _CDump(**{k: a.ctypes.data for k, a in arrs.items()})
+    _check(load().ha_dump_state_c(ctypes.byref(d)), "ha_dump_state_c")
+    arrs["size_infos"] = arrs["size_infos"].reshape(NSIZES, 8)
+    arrs["sets"] = arrs["sets"].reshape(NSETS, nw)
+    arrs["bits"] = arrs["bits"].reshape(n, sb // 512)
+    arrs["nibbles"] = arrs["nibbles"].reshape(n, sb // 128)
+    arrs["pool_base"] = st["pool_base"]
+    arrs["nsbs"] = n
+    arrs["sb_sz"] = sb
+    return arrs
+
+
+def debug_set_head_lock(size_id: int, held: bool) -> None:
+    """Failure-detection test hook (see ha_debug_set_head_lock_c)."""
+    _check(load().ha_debug_set_head_lock_c(size_id, 1 if held else 0),
+           "ha_debug_set_head_lock_c")
+
+
+def l2_persist(stream=None) -> None:
+    _check(load().ha_l2_persist_c(_stream(stream)), "ha_l2_persist_c")
+
+
+# ---- batch entry points ------------------------------------------------------
+
+def malloc_batch(sizes, nthreads: int, nallocs: int, ptrs, tag: bool = False,
+                 stream=None) -> None:
+    _check(load().ha_malloc_batch_c(_addr(sizes), nthreads, nallocs, _addr(ptrs),
+                                    1 if tag else 0, _stream(stream)), "ha_malloc_batch_c")
+
+
+def free_batch(ptrs, nthreads: int, nallocs: int, stream=None) -> None:
+    _check(load().ha_free_batch_c(_addr(ptrs), nthreads, nallocs, _stream(stream)),
+           "ha_free_batch_c")
+
+
+def throughput(out, nthreads: int, nbytes: int = 16, block: int = 128, nallocs: int = 1,
+               niters: int = 1, sizes=None, stream=None) -> None:
+    _check(load().ha_throughput_c(_addr(sizes), nbytes, nthreads, block, nallocs, niters,
+                                  _addr(out), _stream(stream)), "ha_throughput_c")
+
+
+def cuda_throughput(out, nthreads: int, nbytes: int = 16, block: int = 128, nallocs: int = 1,
+                    niters: int = 1, sizes=None, stream=None) -> None:
+    _check(load().ha_cuda_throughput_c(_addr(sizes), nbytes, nthreads, block, nallocs, niters,
+                                       _addr(out), _stream(stream)), "ha_cuda_throughput_c")
+
+
+def throughput_host(h_out: np.ndarray, d_out, nthreads: int, nbytes: int = 16,
+                    block: int = 128, nallocs: int = 1, niters: int = 1, h_sizes=None,
+                    d_sizes=None, stream=None) -> None:
+    """End-to-end form: host sizes in, host (checksum, nfail) out."""
+    _check(load().ha_throughput_host_c(_addr(h_sizes), _addr(d_sizes), nbytes, nthreads,
+                                       block, nallocs, niters, _addr(d_out), _addr(h_out),
+                                       _stream(stream)), "ha_throughput_host_c")
+
+
+def trace(ops, n: int, out, stream=None) -> None:
+    _check(load().ha_trace_c(_addr(ops), n, _addr(out), _stream(stream)), "ha_trace_c")
+
+
+def atomic_peak(buf, nwords: int, nthreads: int, reps: int, returning: bool,
+                stream=None) -> None:
+    _check(load().ha_atomic_peak_c(_addr(buf), nwords, nthreads, reps,
+                                   1 if returning else 0, _stream(stream)), "ha_atomic_peak_c")

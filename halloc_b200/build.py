@@ -1,0 +1,86 @@
+"""Builds halloc-b200 for sm_100a, in-tree.
+
+Outputs (all git-ignored, all travel with the source tree):
+
+* ``halloc_b200/libhalloc.a``       -- relocatable-device-code static library
+  with hamalloc/hafree/ha_init/...: the drop-in for halloc's libhalloc.a.
+  Users compile with ``-rdc=true`` and link it (include/halloc.h).
+* ``halloc_b200/libhalloc_b200.so`` -- the same allocator plus the batch
+  kernels, device-linked, exporting the C ABI of include/halloc_c.h.
+
+Run ``python -m halloc_b200.build`` (or ``__graft_entry__.build()``).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+BUILD = os.path.join(PKG, "_build")
+SO = os.path.join(PKG, "libhalloc_b200.so")
+LIB_A = os.path.join(PKG, "libhalloc.a")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler", "-fPIC",
+                  "-I" + INCLUDE, "-I" + CSRC]
+
+HEADERS = [os.path.join(CSRC, f) for f in ("ha_core.cuh", "ha_types.h")] + [
+    os.path.join(INCLUDE, f) for f in ("halloc.h", "halloc_c.h")]
+SOURCES = ["halloc.cu", "ha_kernels.cu"]
+
+
+def nvcc() -> str:
+    env = os.environ.get("NVCC")
+    if env:
+        return env
+    for cand in ("/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise FileNotFoundError("nvcc not found")
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Compiles what is out of date; returns the path of the shared library."""
+    os.makedirs(BUILD, exist_ok=True)
+    cc = nvcc()
+    objs = []
+    for src in SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        if _stale(o, [s, __file__] + HEADERS) or ptxas_info:
+            extra = ["-Xptxas", "-v"] if ptxas_info else []
+            _run([cc] + CUFLAGS + extra + ["-c", s, "-o", o], verbose)
+        objs.append(o)
+    halloc_o = objs[0]
+    if _stale(LIB_A, [halloc_o]):
+        _run([cc] + ARCH + ["-lib", halloc_o, "-o", LIB_A], verbose)
+    dlink = os.path.join(BUILD, "dlink.o")
+    if _stale(SO, objs):
+        _run([cc] + ARCH + ["-Xcompiler", "-fPIC", "-dlink"] + objs + ["-o", dlink], verbose)
+        _run([cc] + ARCH + ["-shared", "-Xcompiler", "-fPIC"] + objs + [dlink, "-o", SO,
+                                                                         "-lcudadevrt"],
+             verbose)
+    return SO
+
+
+if __name__ == "__main__":
+    build(verbose=True, ptxas_info="--ptxas" in sys.argv)
+    print(SO)

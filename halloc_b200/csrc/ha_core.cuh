@@ -1,0 +1,626 @@
+// ha_core.cuh -- device core of the halloc-b200 small-block allocator.
+//
+// Policy: halloc 0.11's slab/hash policy, step for step (size classes,
+// per-size tickets, hashed first probe, probe sequence, packed slab
+// counters, roomy/sparse/free/busy slab sets, head and cached-head slabs).
+// A single thread calling hamalloc/hafree gets exactly the reference's
+// address sequence.  Mechanism: rebuilt for sm_100a:
+//   * warp aggregation with __match_any_sync / __reduce_add_sync under
+//     explicit member masks, safe under independent thread scheduling;
+//   * explicit PTX memory semantics: .relaxed.gpu atomics on the hot path,
+//     acquire/release on locks and on head publication;
+//   * every wait is bounded by %globaltimer and reports a status bit
+//     instead of spinning forever;
+//   * one contiguous, slab-aligned pool: pointer -> slab is a shift and a
+//     range check (no address grid to read);
+//   * block-size nibbles indexed by in-slab offset / 16, so hafree reads the
+//     nibble and the slab descriptor in parallel;
+//   * slab sets carry a one-word-per-32-words summary so a search touches
+//     two words whatever the pool size.
+//
+// Everything here is internal; the public entry points are hamalloc/hafree
+// (halloc.cu) with the unchanged halloc.h signatures.
+#pragma once
+
+#include <cuda/atomic>
+#include <stdint.h>
+
+#include "ha_types.h"
+
+namespace ha {
+
+// ---------------------------------------------------------------------------
+// device state (defined once, in halloc.cu)
+// ---------------------------------------------------------------------------
+extern __constant__ Config c_cfg;
+extern __device__ Class g_cls[kNSizes];
+extern __device__ State g_st;
+
+// ---------------------------------------------------------------------------
+// PTX helpers: explicit scope and ordering
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t lane_id() {
+  uint32_t l;
+  asm("mov.u32 %0, %%laneid;" : "=r"(l));
+  return l;
+}
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(uint32_t *p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t atom_add(uint32_t *p, uint32_t v) {
+  uint32_t o;
+  asm volatile("atom.relaxed.gpu.global.add.u32 %0, [%1], %2;"
+               : "=r"(o) : "l"(p), "r"(v) : "memory");
+  return o;
+}
+__device__ __forceinline__ uint32_t atom_or(uint32_t *p, uint32_t v) {
+  uint32_t o;
+  asm volatile("atom.relaxed.gpu.global.or.b32 %0, [%1], %2;"
+               : "=r"(o) : "l"(p), "r"(v) : "memory");
+  return o;
+}
+__device__ __forceinline__ uint32_t atom_and(uint32_t *p, uint32_t v) {
+  uint32_t o;
+  asm volatile("atom.relaxed.gpu.global.and.b32 %0, [%1], %2;"
+               : "=r"(o) : "l"(p), "r"(v) : "memory");
+  return o;
+}
+__device__ __forceinline__ void red_add(uint32_t *p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_or(uint32_t *p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_and(uint32_t *p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.and.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// status, bounded waits, locks
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void raise_status(uint32_t bit) {
+  if (!(ld_relaxed(&g_st.status) & bit)) red_or(&g_st.status, bit);
+}
+
+// A wait that gives up after g_st.wait_limit_ns of %globaltimer time.
+struct Deadline {
+  uint64_t end;
+  uint32_t polls;
+  __device__ __forceinline__ Deadline() : end(0), polls(0) {}
+  // true once the limit has passed; checks the clock every 16 polls
+  __device__ __forceinline__ bool expired() {
+    if ((++polls & 15u) != 0) return false;
+    uint64_t now = globaltimer_ns();
+    if (end == 0) {
+      end = now + 1000ull * ld_relaxed(&g_st.wait_limit_us);
+      return false;
+    }
+    return now >= end;
+  }
+  __device__ __forceinline__ void backoff() {
+    __nanosleep(polls < 64 ? 32 : 256);
+  }
+};
+
+__device__ __forceinline__ bool try_lock(uint32_t *m) {
+  cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(*m);
+  return a.exchange(1u, cuda::memory_order_acquire) == 0u;
+}
+// Acquires a one-word lock; false (and HA_ST_TIMEOUT raised) when the wait
+// limit passes first.
+__device__ __forceinline__ bool lock(uint32_t *m) {
+  Deadline d;
+  while (!try_lock(m)) {
+    if (d.expired()) {
+      raise_status(HA_ST_TIMEOUT);
+      return false;
+    }
+    d.backoff();
+  }
+  return true;
+}
+__device__ __forceinline__ void unlock(uint32_t *m) {
+  cuda::atomic_ref<uint32_t, cuda::thread_scope_device> a(*m);
+  a.store(0u, cuda::memory_order_release);
+}
+
+// ---------------------------------------------------------------------------
+// size classes and chunk arithmetic
+// ---------------------------------------------------------------------------
+
+// bytes -> size class 0..15: blocks are 2 or 3 units of 8 << k bytes
+// (the class rule of halloc src/halloc.cu:53-67)
+__device__ __forceinline__ uint32_t size_class(uint32_t n) {
+  n = n < kMinBlock ? kMinBlock : n;
+  uint32_t k = (32u - __clz(n)) - 5u, unit = 8u << k;
+  if (n > 3u * unit) {
+    k++;
+    unit <<= 1;
+  }
+  return 2u * k + (n > 2u * unit ? 1u : 0u);
+}
+// tickets that share one hash slot (src/halloc.cu:101-104)
+__device__ __forceinline__ uint32_t tickets_per_slot(uint32_t sid) {
+  return sid < 2 ? 4u : sid < 4 ? 2u : 1u;
+}
+__device__ __forceinline__ Class load_class(uint32_t sid) {
+  const uint4 *p = reinterpret_cast<const uint4 *>(&g_cls[sid]);
+  uint4 a = __ldg(p), b = __ldg(p + 1);
+  Class c;
+  c.nchunks = a.x;
+  c.chunk_enc = a.y;
+  c.chunk_id = a.z;
+  c.ncib = a.w;
+  c.sparse = b.x;
+  c.hash_step = b.y;
+  c.roomy = b.z;
+  c.busy = b.w;
+  return c;
+}
+// encoded chunk size: (3 or 1) << 16 | shift (halloc src/size-info.h:50-70)
+__device__ __forceinline__ uint32_t chunk_mul(uint32_t v, uint32_t enc) {
+  return (v << (enc & 0xffffu)) * (enc >> 16);
+}
+__device__ __forceinline__ uint32_t chunk_div(uint32_t v, uint32_t enc) {
+  if ((enc >> 16) == 3u) v /= 3u;
+  return v >> (enc & 0xffffu);
+}
+
+// ---------------------------------------------------------------------------
+// slab accessors
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t *ctr_of(uint32_t sb) { return &g_st.ctr[sb * kCtrStride]; }
+__device__ __forceinline__ uint32_t used_of(uint32_t sb) {
+  return ld_relaxed(ctr_of(sb)) >> kCntShift;
+}
+__device__ __forceinline__ uint32_t *bits_of(uint32_t sb) {
+  return c_cfg.bits + ((size_t)sb << c_cfg.bit_words_sh);
+}
+__device__ __forceinline__ uint32_t *nibs_of(uint32_t sb) {
+  return c_cfg.nibs + ((size_t)sb << c_cfg.nib_words_sh);
+}
+__device__ __forceinline__ char *slab_ptr(uint32_t sb) {
+  return c_cfg.pool + ((size_t)sb << c_cfg.sb_sh);
+}
+
+// ---------------------------------------------------------------------------
+// slab sets: atomic bitsets with a summary word per 32 set words
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t *set_words(uint32_t k) { return g_st.sets[k]; }
+__device__ __forceinline__ uint32_t *set_sums(uint32_t k) { return g_st.sums[k]; }
+
+// The word is written before the summary bit, with a fence between, and
+// set_tidy clears the summary bit before re-reading the word, with a fence
+// between: a tidy that clears a summary bit set by a concurrent put is
+// ordered after that put's word write and therefore sees it and restores
+// the bit.  Summary bits may be stale-set (harmless), never stale-clear.
+__device__ __forceinline__ void set_put(uint32_t k, uint32_t sb) {
+  uint32_t w = sb >> 5;
+  red_or(&set_words(k)[w], 1u << (sb & 31));
+  fence_acq_rel();
+  red_or(&set_sums(k)[w >> 5], 1u << (w & 31));
+}
+// Clears the summary bit of word w if the word is empty.
+__device__ __forceinline__ void set_tidy(uint32_t k, uint32_t w) {
+  uint32_t sbit = 1u << (w & 31);
+  atom_and(&set_sums(k)[w >> 5], ~sbit);
+  fence_acq_rel();
+  if (ld_relaxed(&set_words(k)[w])) red_or(&set_sums(k)[w >> 5], sbit);
+}
+__device__ __forceinline__ void set_drop(uint32_t k, uint32_t sb) {
+  uint32_t w = sb >> 5, bit = 1u << (sb & 31);
+  uint32_t old = atom_and(&set_words(k)[w], ~bit);
+  if ((old & ~bit) == 0) set_tidy(k, w);
+}
+// Removes and returns the lowest slab of set k, or kNone
+// (the search order of halloc src/sbset.cuh:5-35).
+__device__ __noinline__ uint32_t set_take(uint32_t k) {
+  uint32_t *sums = set_sums(k), *words = set_words(k);
+  for (uint32_t s = 0; s < c_cfg.sum_words; s++) {
+    uint32_t sw = ld_relaxed(&sums[s]);
+    while (sw) {
+      uint32_t w = s * 32 + (__ffs(sw) - 1);
+      sw &= sw - 1;
+      uint32_t word = ld_relaxed(&words[w]);
+      while (word) {
+        uint32_t b = __ffs(word) - 1, bit = 1u << b;
+        uint32_t old = atom_and(&words[w], ~bit);
+        if (old & bit) {
+          if ((old & ~bit) == 0) set_tidy(k, w);
+          return w * 32 + b;
+        }
+        word = old & ~bit;
+      }
+      set_tidy(k, w);
+    }
+  }
+  return kNone;
+}
+
+// ---------------------------------------------------------------------------
+// slab state transitions (single lane; called by group leaders)
+// ---------------------------------------------------------------------------
+
+// Returns a slab with no used chunks to the free set, or, when detaching a
+// head that still has chunks in use, files it as sparse.  Caller holds the
+// slab lock.  (halloc src/slab.cuh:89-113)
+__device__ __noinline__ void try_release(uint32_t sb, uint32_t cid, bool from_head) {
+  Desc *d = &g_st.desc[sb];
+  if (ld_relaxed(&d->is_head) || cid == kNone) return;
+  uint32_t *c = ctr_of(sb);
+  const uint32_t clear = ((kNone - cid) & kChunkField) << kChunkShift;
+  for (uint32_t guard = 0;; guard++) {
+    uint32_t before = atom_add(c, clear);  // chunk field := none
+    if ((before >> kCntShift) == 0) {
+      st_relaxed(&d->size_id, kNone);
+      st_relaxed(&d->chunk_id, kNone);
+      st_relaxed(&d->chunk_enc, 0);
+      set_put(kSetFree, sb);
+      fence_acq_rel();
+      if (!from_head) set_drop(kSetSparse + cid, sb);
+      return;
+    }
+    uint32_t again = atom_add(c, 0u - clear);  // chunk field restored
+    if ((again >> kCntShift) != 0 || guard > 1024) break;
+  }
+  if (from_head) set_put(kSetSparse + cid, sb);
+}
+
+// Moves a non-head slab between the busy / roomy / sparse / free sets after
+// its count dropped from n0 to n1 (halloc src/slab.cuh:161-224).
+__device__ __noinline__ void file_after_free(uint32_t sb, uint32_t before, uint32_t change) {
+  if (before & kHeadFlag) return;
+  Desc *d = &g_st.desc[sb];
+  uint32_t sid = ld_relaxed(&d->size_id), cid = ld_relaxed(&d->chunk_id);
+  if (sid == kNone || cid == kNone) return;
+  Class cl = load_class(sid);
+  uint32_t n0 = before >> kCntShift, n1 = n0 - change;
+  if (n1 <= cl.busy && n0 > cl.busy) {
+    set_put(kSetBusy + sid, sb);
+  } else if (n1 <= cl.roomy && n0 > cl.roomy) {
+    set_put(kSetRoomy + sid, sb);
+    fence_acq_rel();
+    set_drop(kSetBusy + sid, sb);
+    set_put(kSetRoomy + sid, sb);
+  } else if (n1 <= cl.sparse && n0 > cl.sparse) {
+    set_put(kSetSparse + cid, sb);
+    fence_acq_rel();
+    set_drop(kSetRoomy + sid, sb);
+    set_put(kSetSparse + cid, sb);
+  } else if (n1 == 0 && ((before >> kChunkShift) & kChunkField) != kChunkField) {
+    if (lock(&g_st.sb_lock[sb])) {
+      try_release(sb, ld_relaxed(&d->chunk_id), false);
+      unlock(&g_st.sb_lock[sb]);
+    }
+  }
+}
+
+// Removes `n` chunks from slab sb's count, aggregated over the calling lanes
+// in `mask` that name the same slab; the group leader files the slab.
+__device__ __forceinline__ void count_down(uint32_t mask, uint32_t sb, uint32_t n) {
+  uint32_t grp = __match_any_sync(mask, sb);
+  uint32_t total = __reduce_add_sync(grp, n);
+  if (lane_id() == (uint32_t)(__ffs(grp) - 1)) {
+    uint32_t before = atom_add(ctr_of(sb), 0u - (total << kCntShift));
+    file_after_free(sb, before, total);
+  }
+}
+
+// Stops using `sb` as head and files it by occupancy.  Caller holds the slab
+// lock.  The first comparison uses the ROOMY threshold of the slab's size and
+// the next two read the size-table entry whose index equals the chunk id;
+// both are the reference's rules (halloc src/slab.cuh:227-255) and are kept
+// for identical set contents.
+__device__ __noinline__ void detach(uint32_t sb) {
+  Desc *d = &g_st.desc[sb];
+  st_relaxed(&d->is_head, 0);
+  uint32_t before = atom_add(ctr_of(sb), 0u - kHeadFlag);
+  uint32_t n = before >> kCntShift;
+  uint32_t sid = ld_relaxed(&d->size_id);
+  if (sid >= kNSizes || n > load_class(sid).roomy) return;
+  uint32_t cid = ld_relaxed(&d->chunk_id);
+  if (n == 0) {
+    try_release(sb, cid, true);
+    return;
+  }
+  if (cid >= kNChunkIds) return;
+  Class q = load_class(cid);
+  if (n <= q.sparse)
+    set_put(kSetSparse + cid, sb);
+  else if (n <= q.roomy)
+    set_put(kSetRoomy + sid, sb);
+  else
+    set_put(kSetBusy + sid, sb);
+}
+
+__device__ __forceinline__ void make_head(uint32_t sb) {
+  st_relaxed(&g_st.desc[sb].is_head, 1);
+  red_add(ctr_of(sb), kHeadFlag);
+}
+
+// Picks the next head slab for a size: roomy slabs of the size, sparse slabs
+// of its chunk size, free slabs, then busy slabs at most half way from busy
+// to full (halloc src/slab.cuh:259-372).  kNone if there is none, or if a
+// slab lock could not be taken in time (the slab goes back to its set).
+__device__ __noinline__ uint32_t find_slab(uint32_t sid) {
+  const Class c = load_class(sid);
+  const uint32_t cid = c.chunk_id;
+  uint32_t sb;
+  while ((sb = set_take(kSetRoomy + sid)) != kNone) {
+    if (!lock(&g_st.sb_lock[sb])) {
+      set_put(kSetRoomy + sid, sb);
+      return kNone;
+    }
+    Desc *d = &g_st.desc[sb];
+    bool found = false;
+    if (!ld_relaxed(&d->is_head) && ld_relaxed(&d->size_id) == sid) {
+      if (used_of(sb) <= c.roomy) {
+        found = true;
+        make_head(sb);
+      } else {
+        set_put(kSetBusy + sid, sb);
+      }
+    }
+    unlock(&g_st.sb_lock[sb]);
+    if (found) return sb;
+  }
+  while ((sb = set_take(kSetSparse + cid)) != kNone) {
+    if (!lock(&g_st.sb_lock[sb])) {
+      set_put(kSetSparse + cid, sb);
+      return kNone;
+    }
+    Desc *d = &g_st.desc[sb];
+    bool found = false;
+    if (!ld_relaxed(&d->is_head) && ld_relaxed(&d->chunk_id) == cid) {
+      if (used_of(sb) <= c.sparse) {
+        found = true;
+        make_head(sb);
+        st_relaxed(&d->size_id, sid);
+      } else {
+        uint32_t other = ld_relaxed(&d->size_id);
+        if (other < kNSizes) set_put(kSetRoomy + other, sb);
+      }
+    }
+    unlock(&g_st.sb_lock[sb]);
+    if (found) return sb;
+  }
+  while ((sb = set_take(kSetFree)) != kNone) {
+    if (!lock(&g_st.sb_lock[sb])) {
+      set_put(kSetFree, sb);
+      return kNone;
+    }
+    Desc *d = &g_st.desc[sb];
+    bool found = false;
+    if (!ld_relaxed(&d->is_head)) {
+      found = true;
+      st_relaxed(&d->size_id, sid);
+      st_relaxed(&d->chunk_id, cid);
+      st_relaxed(&d->chunk_enc, c.chunk_enc);
+      make_head(sb);
+      red_add(ctr_of(sb), 0u - (((kNone - cid) & kChunkField) << kChunkShift));
+    }
+    unlock(&g_st.sb_lock[sb]);
+    if (found) return sb;
+  }
+  while ((sb = set_take(kSetBusy + sid)) != kNone) {
+    if (used_of(sb) > (c.busy + c.nchunks) / 2) continue;
+    if (!lock(&g_st.sb_lock[sb])) {
+      set_put(kSetBusy + sid, sb);
+      return kNone;
+    }
+    Desc *d = &g_st.desc[sb];
+    bool found = false;
+    if (!ld_relaxed(&d->is_head) && ld_relaxed(&d->size_id) == sid) {
+      found = true;
+      make_head(sb);
+    }
+    unlock(&g_st.sb_lock[sb]);
+    if (found) return sb;
+  }
+  return kNone;
+}
+
+// Gives size `sid` a new head slab once the current one has reached the busy
+// threshold: the prefetched ("cached") slab first, then a search; the next
+// slab is prefetched right away.  One lane per warp calls this.  A caller
+// that loses the race for the size's lock waits (bounded) until the head
+// changes or the lock is released (halloc src/slab.cuh:378-445).
+__device__ __noinline__ uint32_t replace_head(uint32_t sid) {
+  uint32_t *head = &g_st.head[sid];
+  uint32_t *hlock = &g_st.head_lock[sid * kTicketStride];
+  uint32_t seen = ld_relaxed(head);
+  if (try_lock(hlock)) {
+    uint32_t cur = ld_relaxed(head);
+    uint32_t next;
+    if (cur == kNone || used_of(cur) >= load_class(sid).busy) {
+      next = ld_relaxed(&g_st.cached[sid]);
+      st_relaxed(&g_st.cached[sid], kNone);
+      if (next == kNone) next = find_slab(sid);
+      if (next != kNone) {
+        st_release(head, next);
+        red_add(&g_st.n_head_changes, 1);
+        if (cur != kNone) {
+          if (lock(&g_st.sb_lock[cur])) {
+            detach(cur);
+            unlock(&g_st.sb_lock[cur]);
+          }
+        }
+        st_relaxed(&g_st.cached[sid], find_slab(sid));
+      }
+    } else {
+      next = ld_relaxed(head);
+    }
+    unlock(hlock);
+    return next;
+  }
+  Deadline dl;
+  for (;;) {
+    if (ld_relaxed(head) != seen || ld_relaxed(hlock) == 0) break;
+    if (dl.expired()) {
+      raise_status(HA_ST_TIMEOUT);
+      return kNone;
+    }
+    dl.backoff();
+  }
+  return ld_relaxed(head);
+}
+
+// ---------------------------------------------------------------------------
+// allocation
+// ---------------------------------------------------------------------------
+
+// first probe position of a ticket: tickets_per_slot consecutive tickets
+// share a slot, slots are kHashFreq blocks apart, 32-bit wraparound
+// (halloc src/halloc.cu:107-122)
+__device__ __forceinline__ uint32_t first_probe(const Class &c, uint32_t sid, uint32_t t) {
+  uint32_t low = tickets_per_slot(sid) - 1;
+  uint32_t spread = (t & ~low) * kHashFreq + (t & low);
+  return spread * c.ncib % c.nchunks;
+}
+
+// Small-block allocation for every lane of the calling warp that is active
+// here; lanes may ask for different sizes.  (halloc src/halloc.cu:125-182
+// and src/slab.cuh:453-535, with the warp protocol rebuilt on explicit
+// masks.)
+__device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
+  const uint32_t warp = __activemask();
+  const uint32_t me = lane_id();
+  const uint32_t sid = size_class(nbytes);
+  const Class c = load_class(sid);
+  uint32_t sb = ld_relaxed(&g_st.head[sid]);
+
+  // ticket: consecutive values for lanes of one size, in lane order
+  uint32_t ticket;
+  {
+    uint32_t grp = __match_any_sync(warp, sid);
+    uint32_t lead = __ffs(grp) - 1, base = 0;
+    if (me == lead) base = atom_add(&g_st.ticket[sid * kTicketStride], __popc(grp));
+    base = __shfl_sync(grp, base, lead);
+    ticket = base + __popc(grp & lanemask_lt());
+  }
+  const uint32_t first = first_probe(c, sid, ticket);
+  const uint32_t block = (1u << c.ncib) - 1u;
+
+  void *p = nullptr;
+  bool want = true;
+  uint32_t round = 0, rounds_total = 0;
+  do {
+    bool need_head = false;
+    const uint32_t want_mask = __ballot_sync(warp, want);
+    if (want) {
+      // -- probe the head slab (per lane, no warp ops inside) --------------
+      bool reserved = false;
+      uint32_t pos = first;
+      if (sb == kNone) {
+        need_head = true;
+      } else {
+        uint32_t *bits = bits_of(sb);
+        do {
+          uint32_t mask = block << (pos & 31);
+          uint32_t old = atom_or(&bits[pos >> 5], mask);
+          if (!(old & mask)) {
+            reserved = true;
+            break;
+          }
+          if (~old & mask) red_and(&bits[pos >> 5], ~mask | (old & mask));
+          if (round % kCountCheck == kCountCheck - 1 && used_of(sb) >= c.busy) break;
+          uint32_t k = round + 1;
+          uint32_t step = k * kStepScale * c.ncib % c.hash_step;
+          pos = (first + k * step) % c.nchunks;
+        } while (++round % kTriesPerRound < kTriesPerRound - 1);
+        if (!reserved) need_head = true;
+      }
+      // -- count the reservation, aggregated per slab ----------------------
+      const uint32_t rmask = __ballot_sync(want_mask, reserved);
+      if (reserved) {
+        uint32_t grp = __match_any_sync(rmask, sb);
+        uint32_t total = __reduce_add_sync(grp, c.ncib);
+        uint32_t lead = __ffs(grp) - 1, before = 0;
+        if (me == lead) before = atom_add(ctr_of(sb), total << kCntShift);
+        before = __shfl_sync(grp, before, lead);
+        const bool ok = ((before >> kChunkShift) & kChunkField) == c.chunk_id;
+        const uint32_t n0 = before >> kCntShift;
+        const uint32_t cmask = __ballot_sync(rmask, !ok);
+        if (!ok) {
+          // the slab changed chunk size under us: give the block back
+          red_and(&bits_of(sb)[pos >> 5], ~(block << (pos & 31)));
+          count_down(cmask, sb, c.ncib);
+          need_head = true;
+        } else {
+          if (n0 + total >= c.busy && n0 < c.busy) need_head = true;
+          uint32_t off = chunk_mul(pos, c.chunk_enc);
+          red_or(&nibs_of(sb)[off >> 7], c.ncib << ((off >> 2) & 28));
+          p = slab_ptr(sb) + off;
+          want = false;
+        }
+      }
+    }
+    // -- new head slabs, one lane per size at a time ------------------------
+    uint32_t nmask = __ballot_sync(warp, need_head);
+    while (nmask) {
+      const uint32_t lead = __ffs(nmask) - 1;
+      const uint32_t lsid = __shfl_sync(warp, sid, lead);
+      uint32_t nsb = 0;
+      if (me == lead) nsb = replace_head(sid);
+      nsb = __shfl_sync(warp, nsb, lead);
+      if (need_head && sid == lsid) {
+        sb = nsb;
+        need_head = false;
+        if (nsb == kNone) want = false;
+      }
+      nmask = __ballot_sync(warp, need_head);
+    }
+    if (want && ++rounds_total > kMaxRounds) {
+      raise_status(HA_ST_LIVELOCK);
+      want = false;
+    }
+  } while (__any_sync(warp, want));
+  if (!p) red_add(&g_st.n_null, 1);
+  return p;
+}
+
+// Small-block free for every active lane of the calling warp; `off` is the
+// block's offset from the start of the pool.  (halloc src/halloc.cu:211-230)
+// Block starts are at least 16 B apart (24-B chunks start on 8-B
+// boundaries), so in-slab offset / 16 names a block start uniquely.
+__device__ __forceinline__ void free_small(uint64_t off) {
+  const uint32_t sb = (uint32_t)(off >> c_cfg.sb_sh);
+  const uint32_t in = (uint32_t)off & ((1u << c_cfg.sb_sh) - 1u);
+  // independent loads: the block's nibble (taken and cleared) and the
+  // slab's chunk size
+  uint32_t *nw = &nibs_of(sb)[in >> 7];
+  const uint32_t sh = (in >> 2) & 28;
+  const uint32_t enc = ld_relaxed(&g_st.desc[sb].chunk_enc);
+  const uint32_t old = atom_and(nw, ~(15u << sh));
+  const uint32_t n = (old >> sh) & 15u;
+  bool valid = n != 0 && enc != 0;
+  if (!valid) raise_status(HA_ST_BAD_FREE);
+  const uint32_t ichunk = valid ? chunk_div(in, enc) : 0;
+  if (valid) red_and(&bits_of(sb)[ichunk >> 5], ~(((1u << n) - 1u) << (ichunk & 31)));
+  const uint32_t active = __activemask();
+  const uint32_t vmask = __ballot_sync(active, valid);
+  if (valid) count_down(vmask, sb, n);
+}
+
+}  // namespace ha

@@ -1,0 +1,234 @@
+// ha_kernels.cu -- batch entry points of the C ABI (halloc_c.h).
+//
+// The kernels here are the reference's own test and benchmark kernels
+// (halloc tst/common/common.h:361-412, tst/perf/priv-throughput), written
+// against the public device API: they call hamalloc / hafree across the
+// device-link boundary exactly as a user kernel does.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "halloc.h"
+#include "halloc_c.h"
+
+namespace {
+
+constexpr uint32_t kMaxAllocsPerThread = 16;
+
+cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int launch_status() {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "halloc-b200: launch failed: %s\n", cudaGetErrorString(e));
+    return HA_ECUDA;
+  }
+  return HA_OK;
+}
+
+uint32_t blocks_for(uint64_t n, uint32_t block) { return (uint32_t)((n + block - 1) / block); }
+
+// block-wide sum of two counters, one atomic per block
+__device__ __forceinline__ void block_add2(unsigned long long a, unsigned long long b,
+                                           unsigned long long *out) {
+  __shared__ unsigned long long sa[32], sb[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sa[warp] = a;
+    sb[warp] = b;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t nw = (blockDim.x + 31) >> 5;
+    a = lane < nw ? sa[lane] : 0;
+    b = lane < nw ? sb[lane] : 0;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+      if (a) atomicAdd(&out[0], a);
+      if (b) atomicAdd(&out[1], b);
+    }
+  }
+}
+
+}  // namespace
+
+// malloc_k / malloc_corr_k of halloc tst/common/common.h:361-388
+__global__ void ha_malloc_batch_k(const uint32_t *sizes, uint32_t n, uint32_t nallocs,
+                                  void **ptrs, int tag) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (uint32_t a = 0; a < nallocs; a++) {
+    const size_t k = (size_t)a * n + i;
+    const uint32_t sz = sizes[k];
+    void *p = hamalloc(sz);
+    ptrs[k] = p;
+    if (p && tag) *(uint32_t *)p = sz;
+  }
+}
+
+// free_k of halloc tst/common/common.h:390-399
+__global__ void ha_free_batch_k(void *const *ptrs, uint32_t n, uint32_t nallocs) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (uint32_t a = 0; a < nallocs; a++) hafree(ptrs[(size_t)a * n + i]);
+}
+
+// throughput_malloc_free_k of halloc tst/perf/priv-throughput/priv-throughput.cu:13-27,
+// with the 16-byte payload write and checksummed read-back of each block
+template <bool kCudaHeap>
+__global__ void ha_throughput_k(const uint32_t *sizes, uint32_t nbytes, uint32_t n,
+                                uint32_t nallocs, uint32_t niters,
+                                unsigned long long *out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long sum = 0, nfail = 0;
+  if (i < n) {
+    const uint32_t sz = sizes ? sizes[i] : nbytes;
+    const uint4 word = make_uint4(i ^ 0u, i ^ 1u, i ^ 2u, i ^ 3u);
+    void *ps[kMaxAllocsPerThread];
+    for (uint32_t it = 0; it < niters; it++) {
+      for (uint32_t a = 0; a < nallocs; a++) {
+        void *p = kCudaHeap ? malloc(sz) : hamalloc(sz);
+        ps[a] = p;
+        if (p)
+          *reinterpret_cast<uint4 *>(p) = word;
+        else
+          nfail++;
+      }
+      for (uint32_t a = 0; a < nallocs; a++) {
+        void *p = ps[a];
+        if (!p) continue;
+        const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(p));
+        sum += (unsigned long long)v.x + v.y + v.z + v.w;
+        if (kCudaHeap)
+          free(p);
+        else
+          hafree(p);
+      }
+    }
+  }
+  block_add2(sum, nfail, out);
+}
+
+// serial replay on one thread
+__global__ void ha_trace_k(const int64_t *ops, int64_t n, int64_t *out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int64_t i = 0; i < n; i++) {
+    const int64_t op = ops[i];
+    if (op >= 0) {
+      out[i] = (int64_t)(uintptr_t)hamalloc((size_t)op);
+    } else {
+      hafree((void *)(uintptr_t)out[-(op + 1)]);
+      out[i] = 0;
+    }
+  }
+}
+
+// distinct-address 32-bit atomic OR throughput
+__global__ void ha_atomic_peak_k(uint32_t *buf, uint32_t nwords, uint32_t reps,
+                                 int returning) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t *w = &buf[t % nwords];
+  if (returning) {
+    uint32_t acc0 = 0, acc1 = 0;
+    for (uint32_t r = 0; r < reps; r += 2) {
+      acc0 ^= atomicOr(w, 1u << (r & 31));
+      acc1 ^= atomicOr(w, 2u << (r & 30));
+    }
+    if ((acc0 ^ acc1) == 0x9e3779b9u) buf[0] = acc0;  // keeps the results live
+  } else {
+    for (uint32_t r = 0; r < reps; r++) atomicOr(w, 1u << (r & 31));
+  }
+}
+
+// ---- C ABI ---------------------------------------------------------------
+
+extern "C" int ha_malloc_batch_c(const uint32_t *sizes, uint32_t nthreads, uint32_t nallocs,
+                                 void **ptrs, int tag, void *stream) {
+  if (!sizes || !ptrs || nallocs == 0) return HA_EINVAL;
+  if (nthreads == 0) return HA_OK;
+  ha_malloc_batch_k<<<blocks_for(nthreads, 128), 128, 0, as_stream(stream)>>>(
+      sizes, nthreads, nallocs, ptrs, tag);
+  return launch_status();
+}
+
+extern "C" int ha_free_batch_c(void *const *ptrs, uint32_t nthreads, uint32_t nallocs,
+                               void *stream) {
+  if (!ptrs || nallocs == 0) return HA_EINVAL;
+  if (nthreads == 0) return HA_OK;
+  ha_free_batch_k<<<blocks_for(nthreads, 128), 128, 0, as_stream(stream)>>>(ptrs, nthreads,
+                                                                          nallocs);
+  return launch_status();
+}
+
+static int throughput(bool cuda_heap, const uint32_t *sizes, uint32_t nbytes,
+                      uint32_t nthreads, uint32_t block, uint32_t nallocs, uint32_t niters,
+                      uint64_t *out, void *stream) {
+  if (!out || block == 0 || block > 1024 || nallocs == 0 ||
+      nallocs > kMaxAllocsPerThread)
+    return HA_EINVAL;
+  if (nthreads == 0 || niters == 0) return HA_OK;
+  const uint32_t grid = blocks_for(nthreads, block);
+  unsigned long long *o = reinterpret_cast<unsigned long long *>(out);
+  if (cuda_heap)
+    ha_throughput_k<true><<<grid, block, 0, as_stream(stream)>>>(sizes, nbytes, nthreads,
+                                                               nallocs, niters, o);
+  else
+    ha_throughput_k<false><<<grid, block, 0, as_stream(stream)>>>(sizes, nbytes, nthreads,
+                                                                nallocs, niters, o);
+  return launch_status();
+}
+
+extern "C" int ha_throughput_c(const uint32_t *sizes, uint32_t nbytes, uint32_t nthreads,
+                               uint32_t block, uint32_t nallocs, uint32_t niters,
+                               uint64_t *out, void *stream) {
+  return throughput(false, sizes, nbytes, nthreads, block, nallocs, niters, out, stream);
+}
+
+extern "C" int ha_cuda_throughput_c(const uint32_t *sizes, uint32_t nbytes, uint32_t nthreads,
+                                    uint32_t block, uint32_t nallocs, uint32_t niters,
+                                    uint64_t *out, void *stream) {
+  return throughput(true, sizes, nbytes, nthreads, block, nallocs, niters, out, stream);
+}
+
+extern "C" int ha_throughput_host_c(const uint32_t *h_sizes, uint32_t *d_sizes,
+                                    uint32_t nbytes, uint32_t nthreads, uint32_t block,
+                                    uint32_t nallocs, uint32_t niters, uint64_t *d_out,
+                                    uint64_t *h_out, void *stream) {
+  if (!d_out || !h_out || (h_sizes && !d_sizes)) return HA_EINVAL;
+  cudaStream_t s = as_stream(stream);
+  if (h_sizes &&
+      cudaMemcpyAsync(d_sizes, h_sizes, (size_t)nthreads * 4, cudaMemcpyHostToDevice, s) !=
+          cudaSuccess)
+    return HA_ECUDA;
+  if (cudaMemsetAsync(d_out, 0, 2 * sizeof(uint64_t), s) != cudaSuccess) return HA_ECUDA;
+  int rc = throughput(false, h_sizes ? d_sizes : nullptr, nbytes, nthreads, block, nallocs,
+                      niters, d_out, stream);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(h_out, d_out, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return HA_ECUDA;
+  return HA_OK;
+}
+
+extern "C" int ha_trace_c(const int64_t *ops, int64_t n, int64_t *out, void *stream) {
+  if (!ops || !out || n < 0) return HA_EINVAL;
+  if (n == 0) return HA_OK;
+  ha_trace_k<<<1, 1, 0, as_stream(stream)>>>(ops, n, out);
+  return launch_status();
+}
+
+extern "C" int ha_atomic_peak_c(uint32_t *buf, uint32_t nwords, uint32_t nthreads,
+                                uint32_t reps, int returning, void *stream) {
+  if (!buf || nwords == 0 || nthreads == 0 || reps == 0) return HA_EINVAL;
+  ha_atomic_peak_k<<<blocks_for(nthreads, 256), 256, 0, as_stream(stream)>>>(buf, nwords, reps,
+                                                                            returning);
+  return launch_status();
+}

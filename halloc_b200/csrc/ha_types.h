@@ -1,0 +1,100 @@
+// ha_types.h -- constants and data layout of the halloc-b200 allocator state.
+//
+// Policy constants keep halloc 0.11's values (src/halloc.cu:38-45,
+// src/slab.h:31-63, src/size-info.h:28-47) because the slab/hash policy, and
+// with it every address a single thread receives, depends on them.  Layout
+// constants (strides, limits) are this implementation's own.
+#pragma once
+
+#include <stdint.h>
+
+#include "halloc_c.h"
+
+namespace ha {
+
+// ---- policy (reference values) -------------------------------------------
+constexpr uint32_t kNSizes = 16;        // 2 sizes per unit x 8 units, 16..3072 B
+constexpr uint32_t kNChunkIds = 4;      // chunk sizes 16, 24, 256, 384 B
+constexpr uint32_t kMinBlock = 16;
+constexpr uint32_t kMaxBlock = 3072;
+constexpr uint32_t kFirstTicket = 0x0B0B0B0Bu;
+constexpr uint32_t kHashFreq = 11;      // hash slots are 11 blocks apart
+constexpr uint32_t kTriesPerRound = 32; // probe round length
+constexpr uint32_t kCountCheck = 2;     // read the slab count every 2nd collision
+constexpr uint32_t kStepScale = 64;     // probe step multiplier
+constexpr uint32_t kNone = 0xffffffffu;
+
+// packed slab counter word: used chunks in bits 12-31, head flag in bit 8,
+// chunk id in bits 5-7 (7 = none), bits 0-4 left at 31
+constexpr uint32_t kCntShift = 12;
+constexpr uint32_t kHeadFlag = 1u << 8;
+constexpr uint32_t kChunkShift = 5;
+constexpr uint32_t kChunkField = 7u;
+constexpr uint32_t kCtrInit = (kChunkField << kChunkShift) | 31u;
+
+// ---- layout (this implementation) ----------------------------------------
+constexpr uint32_t kMaxSlabs = 32768;          // 128 GiB of 4-MiB slabs
+constexpr uint32_t kSetWords = kMaxSlabs / 32;
+constexpr uint32_t kSumWords = kSetWords / 32;
+constexpr uint32_t kSetFree = 0;
+constexpr uint32_t kSetSparse = 1;             // + chunk id
+constexpr uint32_t kSetRoomy = kSetSparse + kNChunkIds;  // + size id
+constexpr uint32_t kSetBusy = kSetRoomy + kNSizes;       // + size id
+constexpr uint32_t kNSets = kSetBusy + kNSizes;
+constexpr uint32_t kTicketStride = 32;  // one 128-B line per size's ticket / lock
+constexpr uint32_t kCtrStride = 8;      // one 32-B sector per slab counter
+constexpr uint32_t kMaxRounds = 1u << 16;  // outer-loop bound of one hamalloc
+constexpr uint32_t kDefaultWaitUs = 1000000;  // 1 s
+
+// size class, 32 bytes, the field order of halloc src/size-info.h:8-26
+struct alignas(32) Class {
+  uint32_t nchunks;    // chunks of this size's chunk size in one slab
+  uint32_t chunk_enc;  // (3 or 1) << 16 | log2 of the power-of-two part
+  uint32_t chunk_id;
+  uint32_t ncib;       // chunks in one block: 1, 2, 4 or 8
+  uint32_t sparse;     // thresholds, in chunks
+  uint32_t hash_step;
+  uint32_t roomy;
+  uint32_t busy;
+};
+
+// slab descriptor
+struct alignas(16) Desc {
+  uint32_t size_id;    // kNone when free
+  uint32_t chunk_id;   // kNone when free
+  uint32_t is_head;
+  uint32_t chunk_enc;  // 0 when free
+};
+
+// read-only after ha_init (constant memory)
+struct Config {
+  char *pool;           // slab i at pool + (i << sb_sh)
+  uint64_t pool_bytes;  // nsbs << sb_sh
+  uint32_t *bits;       // one bit per 16 B of pool, slab after slab
+  uint32_t *nibs;       // one 4-bit block length per 16 B of pool
+  uint32_t nsbs;
+  uint32_t sb_sh;
+  uint32_t bit_words_sh;  // log2(words of bits per slab) = sb_sh - 9
+  uint32_t nib_words_sh;  // log2(words of nibbles per slab) = sb_sh - 7
+  uint32_t set_words;     // ceil(nsbs / 32)
+  uint32_t sum_words;     // ceil(set_words / 32)
+};
+
+// mutable allocator state (global memory, one instance per device)
+struct State {
+  uint32_t ticket[kNSizes * kTicketStride];
+  uint32_t head_lock[kNSizes * kTicketStride];
+  alignas(128) uint32_t head[kNSizes];
+  uint32_t cached[kNSizes];
+  alignas(128) uint32_t status;
+  uint32_t wait_limit_us;
+  uint32_t n_head_changes;
+  uint32_t n_null;
+  alignas(128) uint32_t ctr[kMaxSlabs * kCtrStride];
+  Desc desc[kMaxSlabs];
+  uint32_t sb_lock[kMaxSlabs];
+  uint32_t sets[kNSets][kSetWords];
+  uint32_t sums[kNSets][kSumWords];
+};
+
+}  // namespace ha

@@ -1,0 +1,530 @@
+// halloc.cu -- public entry points of halloc-b200 and its host init layer.
+//
+// Device: hamalloc / hafree with halloc.h's signatures and C++ linkage,
+// resolved at device-link time (-rdc) exactly like the original library.
+// Host: ha_init / ha_shutdown / ha_extfrag (C++ API of halloc.h) and the
+// init / statistics half of the C ABI (halloc_c.h).
+#define HALLOCLIB_COMPILING
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+
+#include "halloc.h"
+#include "halloc_c.h"
+#include "ha_core.cuh"
+
+static_assert(sizeof(halloc_opts_t) == sizeof(ha_opts_c),
+              "halloc_opts_t and ha_opts_c must share one layout");
+static_assert(offsetof(halloc_opts_t, sb_sz_sh) == offsetof(ha_opts_c, sb_sz_sh),
+              "halloc_opts_t and ha_opts_c must share one layout");
+
+namespace ha {
+__constant__ Config c_cfg;
+__device__ Class g_cls[kNSizes];
+__device__ State g_st;
+
+// statistics scratch, written by stats_k
+struct StatsOut {
+  unsigned long long used_chunks, used_bytes, free_bytes, ideal_bytes;
+  unsigned int free_slabs, head_slabs;
+};
+__device__ StatsOut g_stats_out;
+__device__ unsigned long long g_max_alloc;
+}  // namespace ha
+
+// ---------------------------------------------------------------------------
+// device entry points
+// ---------------------------------------------------------------------------
+
+__device__ __noinline__ void *hamalloc(size_t nbytes) {
+  if (nbytes > ha::kMaxBlock) return malloc(nbytes);
+  if (ha::c_cfg.nsbs == 0) return nullptr;  // not initialised
+  return ha::malloc_small((uint32_t)nbytes);
+}
+
+__device__ __noinline__ void hafree(void *p) {
+  if (!p) return;
+  uint64_t off = (uint64_t)((const char *)p - ha::c_cfg.pool);
+  if (off < ha::c_cfg.pool_bytes)
+    ha::free_small(off);
+  else
+    free(p);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+
+struct HostDev {
+  bool init;
+  char *raw_pool;
+  char *pool;
+  uint64_t pool_bytes;
+  uint32_t *meta;
+  size_t meta_bytes;
+  uint64_t heap_bytes;
+  uint32_t nsbs, sb_sh;
+  bool heap_ok;
+  size_t persist_bytes;
+};
+constexpr int kMaxDevices = 64;
+HostDev g_dev[kMaxDevices];
+
+#define HA_CK(call)                                   \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) {                          \
+      fprintf(stderr, "halloc-b200: %s failed: %s\n", \
+              #call, cudaGetErrorString(e_));         \
+      return HA_ECUDA;                                \
+    }                                                 \
+  } while (0)
+
+HostDev *current(int *dev_out = nullptr) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  if (dev_out) *dev_out = dev;
+  return &g_dev[dev];
+}
+
+// largest prime p in [3, n) dividing neither n nor nb; 0 if none
+// (the hash-step rule of halloc src/utils.cu:8-24)
+uint32_t prime_below(uint32_t n, uint32_t nb) {
+  for (uint32_t p = n - 1; p >= 3 && p < n; p--) {
+    bool prime = true;
+    for (uint32_t d = 2; (uint64_t)d * d <= p; d++)
+      if (p % d == 0) {
+        prime = false;
+        break;
+      }
+    if (prime && n % p && nb % p) return p;
+  }
+  return 0;
+}
+
+uint32_t chunk_enc(uint32_t bytes) {
+  uint32_t three = bytes % 3 == 0, base = three ? bytes / 3 : bytes, sh = 0;
+  while ((1u << sh) < base) sh++;
+  return (three ? 3u : 1u) << 16 | sh;
+}
+
+// the size-class table of halloc src/halloc.cu:363-394
+bool build_classes(ha::Class *cls, uint32_t sb_bytes, const ha_opts_c &o) {
+  for (uint32_t sid = 0; sid < ha::kNSizes; sid++) {
+    ha::Class &c = cls[sid];
+    uint32_t unit = 8u << (sid / 2), block = (sid & 1 ? 3 : 2) * unit;
+    uint32_t per_slot = sid < 2 ? 4u : sid < 4 ? 2u : 1u;
+    uint32_t nblocks = sb_bytes / block / per_slot * per_slot;
+    c.chunk_id = (sid & 1) + (sid < ha::kNSizes / 2 ? 0 : 2);
+    uint32_t cbytes = (c.chunk_id & 1 ? 3 : 2) * (c.chunk_id >= 2 ? 128 : 8);
+    c.chunk_enc = chunk_enc(cbytes);
+    c.ncib = block / cbytes;
+    c.nchunks = nblocks * c.ncib;
+    uint32_t p = prime_below(nblocks / 256 + nblocks / 64, nblocks);
+    if (!p) return false;
+    c.hash_step = c.ncib * p;
+    c.roomy = (uint32_t)(o.roomy_fraction * c.nchunks);
+    c.busy = (uint32_t)(o.busy_fraction * c.nchunks);
+    c.sparse = (uint32_t)(o.sparse_fraction * c.nchunks);
+  }
+  return true;
+}
+
+bool valid_fraction(double f) { return f >= 0.0 && f <= 1.0; }
+
+int shutdown_impl() {
+  int dev;
+  HostDev *h = current(&dev);
+  if (!h) return HA_ECUDA;
+  if (!h->init) return HA_ESTATE;
+  HA_CK(cudaDeviceSynchronize());
+  ha::Config zero;
+  memset(&zero, 0, sizeof(zero));
+  HA_CK(cudaMemcpyToSymbol(ha::c_cfg, &zero, sizeof(zero)));
+  HA_CK(cudaFree(h->raw_pool));
+  HA_CK(cudaFree(h->meta));
+  if (h->persist_bytes) {
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+    cudaGetLastError();
+  }
+  memset(h, 0, sizeof(*h));
+  return HA_OK;
+}
+
+int init_impl(const ha_opts_c &o) {
+  int dev;
+  HostDev *h = current(&dev);
+  if (!h) return HA_ECUDA;
+  if (h->init) return HA_ESTATE;
+  if (o.memory == 0 || o.sb_sz_sh < 20 || o.sb_sz_sh > 24 ||
+      !(o.halloc_fraction > 0.0 && o.halloc_fraction <= 1.0) ||
+      !valid_fraction(o.busy_fraction) || !valid_fraction(o.roomy_fraction) ||
+      !valid_fraction(o.sparse_fraction))
+    return HA_EINVAL;
+  cudaDeviceProp prop;
+  HA_CK(cudaGetDeviceProperties(&prop, dev));
+  const uint32_t sb_sh = (uint32_t)o.sb_sz_sh, sb_bytes = 1u << sb_sh;
+  uint64_t memory = o.memory;
+  uint64_t cap = 3ull * prop.totalGlobalMem / 4ull;
+  if (memory > cap) memory = cap;
+  uint64_t slab_mem = (uint64_t)(o.halloc_fraction * (double)memory);
+  uint64_t heap_mem = memory - slab_mem;
+  uint64_t nsbs = slab_mem >> sb_sh;
+  if (nsbs == 0) return HA_EINVAL;
+  if (nsbs > ha::kMaxSlabs) return HA_ERANGE;
+
+  ha::Class cls[ha::kNSizes];
+  if (!build_classes(cls, sb_bytes, o)) return HA_EINVAL;
+
+  // CUDA heap for blocks above 3072 bytes.  The size cannot change once a
+  // kernel of this context has used in-kernel malloc; the allocator still
+  // works then, with the heap it has.
+  bool heap_ok = cudaDeviceSetLimit(cudaLimitMallocHeapSize, heap_mem) == cudaSuccess;
+  cudaGetLastError();
+
+  char *raw = nullptr;
+  uint32_t *meta = nullptr;
+  const uint64_t pool_bytes = nsbs << sb_sh;
+  if (cudaMalloc(&raw, pool_bytes + sb_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return HA_ECUDA;
+  }
+  char *pool = (char *)(((uintptr_t)raw + sb_bytes - 1) & ~(uintptr_t)(sb_bytes - 1));
+  const size_t bit_words = (size_t)nsbs << (sb_sh - 9);
+  const size_t nib_words = (size_t)nsbs << (sb_sh - 7);
+  const size_t meta_bytes = (bit_words + nib_words) * 4;
+  if (cudaMalloc(&meta, meta_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(raw);
+    return HA_ECUDA;
+  }
+  int rc = HA_OK;
+  ha::State *st = new (std::nothrow) ha::State;
+  if (!st) rc = HA_ECUDA;
+  if (rc == HA_OK) {
+    memset(st, 0, sizeof(*st));
+    for (uint32_t s = 0; s < ha::kNSizes; s++) {
+      st->ticket[s * ha::kTicketStride] = ha::kFirstTicket;
+      st->head[s] = ha::kNone;
+      st->cached[s] = ha::kNone;
+    }
+    st->wait_limit_us = ha::kDefaultWaitUs;
+    for (uint32_t sb = 0; sb < nsbs; sb++) {
+      st->ctr[sb * ha::kCtrStride] = ha::kCtrInit;
+      st->desc[sb].size_id = ha::kNone;
+      st->desc[sb].chunk_id = ha::kNone;
+      st->sets[ha::kSetFree][sb >> 5] |= 1u << (sb & 31);
+      st->sums[ha::kSetFree][sb >> 10] |= 1u << ((sb >> 5) & 31);
+    }
+    ha::Config cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.pool = pool;
+    cfg.pool_bytes = pool_bytes;
+    cfg.bits = meta;
+    cfg.nibs = meta + bit_words;
+    cfg.nsbs = (uint32_t)nsbs;
+    cfg.sb_sh = sb_sh;
+    cfg.bit_words_sh = sb_sh - 9;
+    cfg.nib_words_sh = sb_sh - 7;
+    cfg.set_words = (uint32_t)((nsbs + 31) / 32);
+    cfg.sum_words = (cfg.set_words + 31) / 32;
+    if (cudaMemset(meta, 0, meta_bytes) != cudaSuccess ||
+        cudaMemcpyToSymbol(ha::g_cls, cls, sizeof(cls)) != cudaSuccess ||
+        cudaMemcpyToSymbol(ha::g_st, st, sizeof(*st)) != cudaSuccess ||
+        cudaMemcpyToSymbol(ha::c_cfg, &cfg, sizeof(cfg)) != cudaSuccess ||
+        cudaDeviceSynchronize() != cudaSuccess) {
+      cudaGetLastError();
+      rc = HA_ECUDA;
+    }
+  }
+  delete st;
+  if (rc != HA_OK) {
+    cudaFree(raw);
+    cudaFree(meta);
+    return rc;
+  }
+  // persisting-L2 carve-out for the slab metadata (a context limit; it is
+  // released by ha_shutdown and by context teardown)
+  size_t persist = 0;
+  if (prop.persistingL2CacheMaxSize > 0) {
+    persist = meta_bytes < (size_t)prop.persistingL2CacheMaxSize
+                  ? meta_bytes
+                  : (size_t)prop.persistingL2CacheMaxSize;
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist) != cudaSuccess) {
+      cudaGetLastError();
+      persist = 0;
+    }
+  }
+  h->init = true;
+  h->raw_pool = raw;
+  h->pool = pool;
+  h->pool_bytes = pool_bytes;
+  h->meta = meta;
+  h->meta_bytes = meta_bytes;
+  h->heap_bytes = heap_mem;
+  h->nsbs = (uint32_t)nsbs;
+  h->sb_sh = sb_sh;
+  h->heap_ok = heap_ok;
+  h->persist_bytes = persist;
+  return HA_OK;
+}
+
+ha_opts_c to_c(const halloc_opts_t &o) {
+  ha_opts_c c;
+  c.memory = o.memory;
+  c.halloc_fraction = o.halloc_fraction;
+  c.busy_fraction = o.busy_fraction;
+  c.roomy_fraction = o.roomy_fraction;
+  c.sparse_fraction = o.sparse_fraction;
+  c.sb_sz_sh = o.sb_sz_sh;
+  return c;
+}
+
+}  // namespace
+
+// ---- statistics kernels ----------------------------------------------------
+
+// one thread per slab: used chunks/bytes, free and head slabs
+// (the per-slab sum of halloc src/statistics.cuh:34-48, as a reduction)
+__global__ void ha_stats_k(int ideal) {
+  using namespace ha;
+  __shared__ unsigned long long s_chunks, s_bytes, s_free, s_ideal;
+  __shared__ unsigned int s_fslabs, s_hslabs;
+  if (threadIdx.x == 0) {
+    s_chunks = s_bytes = s_free = s_ideal = 0;
+    s_fslabs = s_hslabs = 0;
+  }
+  __syncthreads();
+  uint32_t sb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sb < c_cfg.nsbs) {
+    uint32_t used = ld_relaxed(ctr_of(sb)) >> kCntShift;
+    uint32_t enc = ld_relaxed(&g_st.desc[sb].chunk_enc);
+    uint64_t ubytes = enc ? (uint64_t)chunk_mul(used, enc) : 0;
+    uint64_t sbb = 1ull << c_cfg.sb_sh;
+    atomicAdd(&s_chunks, (unsigned long long)used);
+    atomicAdd(&s_bytes, (unsigned long long)ubytes);
+    atomicAdd(&s_free, (unsigned long long)(sbb - ubytes));
+    if (ideal && enc == 0) atomicAdd(&s_ideal, (unsigned long long)sbb);
+    if ((ld_relaxed(&g_st.sets[kSetFree][sb >> 5]) >> (sb & 31)) & 1u) atomicAdd(&s_fslabs, 1u);
+    if (ld_relaxed(&g_st.desc[sb].is_head)) atomicAdd(&s_hslabs, 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicAdd(&g_stats_out.used_chunks, s_chunks);
+    atomicAdd(&g_stats_out.used_bytes, s_bytes);
+    atomicAdd(&g_stats_out.free_bytes, s_free);
+    atomicAdd(&g_stats_out.ideal_bytes, s_ideal);
+    atomicAdd(&g_stats_out.free_slabs, s_fslabs);
+    atomicAdd(&g_stats_out.head_slabs, s_hslabs);
+  }
+}
+
+// largest block the CUDA heap can give, by bisection on in-kernel malloc
+// (halloc src/statistics.cuh:14-30; like the original it reports the last
+// midpoint tried)
+__global__ void ha_max_alloc_k(unsigned long long heap) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  unsigned long long hi = heap, lo = 0, mid = 0;
+  const unsigned long long step = 1ull << 20;
+  while (hi - lo > step) {
+    mid = (hi + lo) / 2;
+    void *p = malloc(mid);
+    if (p) {
+      lo = mid;
+      free(p);
+    } else {
+      hi = mid;
+    }
+  }
+  ha::g_max_alloc = mid;
+}
+
+namespace {
+int run_stats(int ideal, ha::StatsOut *out) {
+  HostDev *h = current();
+  if (!h) return HA_ECUDA;
+  if (!h->init) return HA_ESTATE;
+  ha::StatsOut zero;
+  memset(&zero, 0, sizeof(zero));
+  HA_CK(cudaMemcpyToSymbol(ha::g_stats_out, &zero, sizeof(zero)));
+  ha_stats_k<<<(h->nsbs + 127) / 128, 128>>>(ideal);
+  HA_CK(cudaGetLastError());
+  HA_CK(cudaMemcpyFromSymbol(out, ha::g_stats_out, sizeof(*out)));
+  return HA_OK;
+}
+}  // namespace
+
+// ---- C++ API (halloc.h) ------------------------------------------------------
+
+void ha_init(halloc_opts_t opts) {
+  HostDev *h = current();
+  if (h && h->init) shutdown_impl();
+  ha_opts_c c = to_c(opts);
+  int rc = init_impl(c);
+  if (rc != HA_OK) {
+    fprintf(stderr, "halloc-b200: ha_init failed (%d)\n", rc);
+    exit(-1);
+  }
+}
+
+void ha_shutdown(void) { shutdown_impl(); }
+
+double ha_extfrag(bool ideal) { return ha_extfrag_c(ideal ? 1 : 0); }
+
+// ---- C ABI: init / stats layer ----------------------------------------------
+
+extern "C" int ha_init_c(const ha_opts_c *opts) {
+  if (!opts) return HA_EINVAL;
+  return init_impl(*opts);
+}
+
+extern "C" int ha_shutdown_c(void) { return shutdown_impl(); }
+
+extern "C" double ha_extfrag_c(int ideal) {
+  HostDev *h = current();
+  if (!h || !h->init) return -1.0;
+  unsigned long long zero = 0;
+  if (cudaMemcpyToSymbol(ha::g_max_alloc, &zero, sizeof(zero)) != cudaSuccess) return -1.0;
+  ha_max_alloc_k<<<1, 32>>>(h->heap_bytes);
+  if (cudaGetLastError() != cudaSuccess) return -1.0;
+  ha::StatsOut s;
+  if (run_stats(ideal, &s) != HA_OK) return -1.0;
+  unsigned long long max_alloc = 0;
+  if (cudaMemcpyFromSymbol(&max_alloc, ha::g_max_alloc, sizeof(max_alloc)) != cudaSuccess)
+    return -1.0;
+  double free_mem = (double)s.free_bytes + (double)h->heap_bytes;
+  double best = (double)max_alloc + (double)s.ideal_bytes;
+  return free_mem > 0 ? 1.0 - best / free_mem : 0.0;
+}
+
+extern "C" int ha_stats_c(ha_stats_t *out) {
+  if (!out) return HA_EINVAL;
+  HostDev *h = current();
+  if (!h) return HA_ECUDA;
+  if (!h->init) return HA_ESTATE;
+  ha::StatsOut s;
+  int rc = run_stats(0, &s);
+  if (rc) return rc;
+  uint32_t head[ha::kNSizes], cached[ha::kNSizes], misc[4];
+  HA_CK(cudaMemcpyFromSymbol(head, ha::g_st, sizeof(head), offsetof(ha::State, head)));
+  HA_CK(cudaMemcpyFromSymbol(cached, ha::g_st, sizeof(cached), offsetof(ha::State, cached)));
+  HA_CK(cudaMemcpyFromSymbol(misc, ha::g_st, sizeof(misc), offsetof(ha::State, status)));
+  memset(out, 0, sizeof(*out));
+  out->pool_base = (uint64_t)(uintptr_t)h->pool;
+  out->pool_bytes = h->pool_bytes;
+  out->cuda_heap_bytes = h->heap_bytes;
+  out->used_chunks = s.used_chunks;
+  out->used_bytes = s.used_bytes;
+  out->nsbs = h->nsbs;
+  out->sb_sz = 1u << h->sb_sh;
+  out->free_slabs = s.free_slabs;
+  out->head_slabs = s.head_slabs;
+  out->status = misc[0];
+  out->n_head_changes = misc[2];
+  out->n_null = misc[3];
+  out->heap_limit_ok = h->heap_ok ? 1 : 0;
+  memcpy(out->head, head, sizeof(head));
+  memcpy(out->cached, cached, sizeof(cached));
+  return HA_OK;
+}
+
+extern "C" uint32_t ha_status_c(void) {
+  uint32_t st = 0;
+  if (cudaMemcpyFromSymbol(&st, ha::g_st, sizeof(st), offsetof(ha::State, status)) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 0xffffffffu;
+  }
+  return st;
+}
+
+extern "C" int ha_clear_status_c(void) {
+  uint32_t z = 0;
+  HA_CK(cudaMemcpyToSymbol(ha::g_st, &z, sizeof(z), offsetof(ha::State, status)));
+  return HA_OK;
+}
+
+extern "C" int ha_set_wait_limit_c(uint32_t microseconds) {
+  if (microseconds == 0) return HA_EINVAL;
+  HA_CK(cudaMemcpyToSymbol(ha::g_st, &microseconds, sizeof(microseconds),
+                           offsetof(ha::State, wait_limit_us)));
+  return HA_OK;
+}
+
+extern "C" int ha_dump_state_c(const ha_state_dump_t *d) {
+  if (!d) return HA_EINVAL;
+  HostDev *h = current();
+  if (!h) return HA_ECUDA;
+  if (!h->init) return HA_ESTATE;
+  HA_CK(cudaDeviceSynchronize());
+  ha::State *st = new (std::nothrow) ha::State;
+  if (!st) return HA_ECUDA;
+  if (cudaMemcpyFromSymbol(st, ha::g_st, sizeof(*st)) != cudaSuccess) {
+    delete st;
+    return HA_ECUDA;
+  }
+  const uint32_t n = h->nsbs, nw = (n + 31) / 32;
+  for (uint32_t s = 0; s < ha::kNSizes; s++) {
+    if (d->tickets) d->tickets[s] = st->ticket[s * ha::kTicketStride];
+    if (d->heads) d->heads[s] = st->head[s];
+    if (d->cached) d->cached[s] = st->cached[s];
+  }
+  for (uint32_t sb = 0; sb < n; sb++) {
+    if (d->counters) d->counters[sb] = st->ctr[sb * ha::kCtrStride];
+    if (d->size_id) d->size_id[sb] = st->desc[sb].size_id;
+    if (d->chunk_id) d->chunk_id[sb] = st->desc[sb].chunk_id;
+    if (d->is_head) d->is_head[sb] = st->desc[sb].is_head;
+    if (d->chunk_enc) d->chunk_enc[sb] = st->desc[sb].chunk_enc;
+  }
+  if (d->sets)
+    for (uint32_t k = 0; k < ha::kNSets; k++)
+      memcpy(d->sets + (size_t)k * nw, st->sets[k], nw * 4);
+  delete st;
+  if (d->size_infos) HA_CK(cudaMemcpyFromSymbol(d->size_infos, ha::g_cls, sizeof(ha::Class) * ha::kNSizes));
+  const size_t bit_words = (size_t)n << (h->sb_sh - 9);
+  const size_t nib_words = (size_t)n << (h->sb_sh - 7);
+  if (d->bits) HA_CK(cudaMemcpy(d->bits, h->meta, bit_words * 4, cudaMemcpyDeviceToHost));
+  if (d->nibbles)
+    HA_CK(cudaMemcpy(d->nibbles, h->meta + bit_words, nib_words * 4, cudaMemcpyDeviceToHost));
+  return HA_OK;
+}
+
+extern "C" int ha_debug_set_head_lock_c(uint32_t size_id, uint32_t held) {
+  if (size_id >= ha::kNSizes || held > 1) return HA_EINVAL;
+  HostDev *h = current();
+  if (!h) return HA_ECUDA;
+  if (!h->init) return HA_ESTATE;
+  HA_CK(cudaDeviceSynchronize());
+  HA_CK(cudaMemcpyToSymbol(ha::g_st, &held, sizeof(held),
+                           offsetof(ha::State, head_lock) +
+                               sizeof(uint32_t) * size_id * ha::kTicketStride));
+  return HA_OK;
+}
+
+extern "C" int ha_l2_persist_c(void *stream) {
+  HostDev *h = current();
+  if (!h) return HA_ECUDA;
+  if (!h->init) return HA_ESTATE;
+  if (!h->persist_bytes) return HA_OK;  // no persisting L2 on this device
+  int dev;
+  HA_CK(cudaGetDevice(&dev));
+  int max_window = 0;
+  HA_CK(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev));
+  cudaStreamAttrValue v;
+  memset(&v, 0, sizeof(v));
+  size_t win = h->meta_bytes < (size_t)max_window ? h->meta_bytes : (size_t)max_window;
+  v.accessPolicyWindow.base_ptr = h->meta;
+  v.accessPolicyWindow.num_bytes = win;
+  v.accessPolicyWindow.hitRatio = win ? (float)fmin(1.0, (double)h->persist_bytes / (double)win) : 0.f;
+  v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+  v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  HA_CK(cudaStreamSetAttribute((cudaStream_t)stream, cudaStreamAttributeAccessPolicyWindow, &v));
+  return HA_OK;
+}

@@ -1,0 +1,175 @@
+#ifndef HALLOC_C_H_
+#define HALLOC_C_H_
+
+/*
+ * halloc_c.h -- C ABI of halloc-b200 (libhalloc_b200.so).
+ *
+ * Plain C types only: device buffers are raw device pointers, streams are
+ * cudaStream_t passed as void* (NULL = the legacy default stream).  Every
+ * int-returning call gives HA_OK (0) or a negative HA_E* code and never
+ * exits the process.
+ *
+ * The allocator itself is used from device code through hamalloc/hafree
+ * (include/halloc.h).  This ABI is the host side of it: the init / stats
+ * layer, and batch entry points that run the reference's own test and
+ * benchmark kernels (malloc a batch, free a batch, the private-throughput
+ * loop) so that a host program -- or a Python/ctypes harness -- can drive
+ * the allocator without compiling device code.
+ */
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes -------------------------------------------------- */
+#define HA_OK 0
+#define HA_EINVAL (-1)   /* invalid argument or option */
+#define HA_ECUDA (-2)    /* a CUDA runtime call failed */
+#define HA_ESTATE (-3)   /* not initialised, or already initialised */
+#define HA_ERANGE (-4)   /* a size beyond a documented limit */
+
+/* ---- device status bits (ha_status_c) ------------------------------ */
+#define HA_ST_TIMEOUT 0x1u  /* a bounded device-side wait gave up */
+#define HA_ST_BAD_FREE 0x2u /* hafree of a pointer that is no live block */
+#define HA_ST_LIVELOCK 0x4u /* a hamalloc exceeded its probe-round bound */
+
+/* Options: same fields, order and layout as struct halloc_opts_t
+   (include/halloc.h; halloc src/halloc.h:15-34). */
+typedef struct ha_opts_c {
+  uint64_t memory;
+  double halloc_fraction;
+  double busy_fraction;
+  double roomy_fraction;
+  double sparse_fraction;
+  int32_t sb_sz_sh;
+} ha_opts_c;
+
+/* ---- init / shutdown / statistics ---------------------------------- */
+
+/* Initialises the allocator on the current device.  HA_ESTATE if it is
+   already initialised there (call ha_shutdown_c first).
+   Replaces ha_init (halloc src/halloc.cu:267-424). */
+int ha_init_c(const ha_opts_c *opts);
+
+/* Frees the allocator's device memory; blocks still held become invalid.
+   Replaces ha_shutdown (halloc src/halloc.cu:426-428, a no-op there). */
+int ha_shutdown_c(void);
+
+/* External fragmentation (see ha_extfrag in include/halloc.h); negative on
+   error.  Replaces ha_extfrag (halloc src/statistics.cuh:50-69). */
+double ha_extfrag_c(int ideal);
+
+typedef struct ha_stats_t {
+  uint64_t pool_base;       /* device address of slab 0 */
+  uint64_t pool_bytes;      /* nsbs * slab size */
+  uint64_t cuda_heap_bytes; /* CUDA heap size requested by init */
+  uint64_t used_chunks;     /* chunks in live small blocks */
+  uint64_t used_bytes;      /* bytes in live small blocks */
+  uint32_t nsbs;
+  uint32_t sb_sz;
+  uint32_t free_slabs;      /* slabs in the free set */
+  uint32_t head_slabs;      /* slabs flagged head (heads + prefetched) */
+  uint32_t status;          /* HA_ST_* bits */
+  uint32_t n_head_changes;  /* head replacements since init */
+  uint32_t n_null;          /* small requests answered with NULL */
+  uint32_t heap_limit_ok;   /* 1 if the CUDA heap size could be set */
+  uint32_t head[16];        /* head slab per size class, 0xffffffff none */
+  uint32_t cached[16];      /* prefetched next head per size class */
+} ha_stats_t;
+
+/* Fills *out (synchronises the device).  No counterpart in the reference,
+   which only had ha_extfrag. */
+int ha_stats_c(ha_stats_t *out);
+
+/* Returns the HA_ST_* bits raised since init / the last clear. */
+uint32_t ha_status_c(void);
+int ha_clear_status_c(void);
+
+/* Bound, in microseconds, of every device-side wait (default 1 s). */
+int ha_set_wait_limit_c(uint32_t microseconds);
+
+/* Full allocator state in host buffers, for parity checks against the host
+   replay model.  NULL members are skipped.  Sizes: tickets/heads/cached 16,
+   size_infos 16*8, per-slab arrays nsbs, sets 37*ceil(nsbs/32) (free,
+   sparse[4], roomy[16], busy[16]), bits nsbs*(slab/512),
+   nibbles nsbs*(slab/128) (4 bits per 16 B of slab, indexed by offset/16). */
+typedef struct ha_state_dump_t {
+  uint32_t *tickets, *heads, *cached, *size_infos;
+  uint32_t *counters, *size_id, *chunk_id, *is_head, *chunk_enc;
+  uint32_t *sets, *bits, *nibbles;
+} ha_state_dump_t;
+int ha_dump_state_c(const ha_state_dump_t *out);
+
+/* Pins the slab metadata (bit arrays, size nibbles) in L2 for kernels
+   launched on `stream` (an access-policy window over the metadata). */
+int ha_l2_persist_c(void *stream);
+
+/* Test hook for failure detection: sets the head-replacement lock of size
+   class `size_id` to `held` (1 = held by a holder that never releases it,
+   0 = free).  A hamalloc that then needs a new head for that size waits
+   until the wait limit, raises HA_ST_TIMEOUT and returns NULL.  No
+   counterpart in the reference (its waits are unbounded). */
+int ha_debug_set_head_lock_c(uint32_t size_id, uint32_t held);
+
+/* ---- batch entry points (device buffers) --------------------------- */
+
+/* Thread i of nthreads performs nallocs hamalloc calls; request a of thread
+   i has size sizes[a*nthreads + i] and its pointer goes to
+   ptrs[a*nthreads + i].  tag != 0 writes the request size into the first
+   4 bytes of each block.  Replaces malloc_k / malloc_corr_k
+   (halloc tst/common/common.h:361-388). */
+int ha_malloc_batch_c(const uint32_t *sizes, uint32_t nthreads,
+                      uint32_t nallocs, void **ptrs, int tag, void *stream);
+
+/* hafree of ptrs[a*nthreads + i] for every thread i and a < nallocs.
+   Replaces free_k (halloc tst/common/common.h:390-399). */
+int ha_free_batch_c(void *const *ptrs, uint32_t nthreads, uint32_t nallocs,
+                    void *stream);
+
+/* The private-throughput loop: nthreads threads in blocks of `block`, each
+   doing niters x (nallocs x hamalloc(sizes[i]); write 16 bytes
+   {i^0,i^1,i^2,i^3} to each block; read them back into a checksum;
+   nallocs x hafree).  sizes may be NULL for a fixed `nbytes`.
+   out[0] += checksum, out[1] += failed allocations (out is not cleared).
+   Replaces throughput_malloc_free_k + PrivThroughputTest
+   (halloc tst/perf/priv-throughput/priv-throughput.cu:13-63). */
+int ha_throughput_c(const uint32_t *sizes, uint32_t nbytes, uint32_t nthreads,
+                    uint32_t block, uint32_t nallocs, uint32_t niters,
+                    uint64_t *out, void *stream);
+
+/* The same loop end to end from host memory: copies h_sizes (nthreads
+   words; NULL for a fixed nbytes) into d_sizes, clears d_out, runs the
+   loop, copies d_out (2 words) to h_out and synchronises the stream. */
+int ha_throughput_host_c(const uint32_t *h_sizes, uint32_t *d_sizes,
+                         uint32_t nbytes, uint32_t nthreads, uint32_t block,
+                         uint32_t nallocs, uint32_t niters, uint64_t *d_out,
+                         uint64_t *h_out, void *stream);
+
+/* The same loop with CUDA's in-kernel malloc/free instead of
+   hamalloc/hafree: the comparator of the reference's benchmarks
+   (halloc tst/common/cuda-malloc-wrapper.h:8-20). */
+int ha_cuda_throughput_c(const uint32_t *sizes, uint32_t nbytes,
+                         uint32_t nthreads, uint32_t block, uint32_t nallocs,
+                         uint32_t niters, uint64_t *out, void *stream);
+
+/* Replays a trace on ONE device thread: op >= 0 is hamalloc(op);
+   op < 0 is hafree of the block returned by op index -(op + 1).
+   out[i] = the pointer hamalloc returned (0 for NULL) as an integer, and 0
+   for a free.  No counterpart in the reference: it exists so that a serial
+   address sequence can be compared with the host replay model. */
+int ha_trace_c(const int64_t *ops, int64_t n, int64_t *out, void *stream);
+
+/* L2 atomic throughput probe: every thread of `nthreads` applies `reps`
+   32-bit atomic ORs to its own word of buf[nwords] (returning != 0 uses
+   the returned value, like a bit-array reservation).  For the roofline
+   denominator; no counterpart in the reference. */
+int ha_atomic_peak_c(uint32_t *buf, uint32_t nwords, uint32_t nthreads,
+                     uint32_t reps, int returning, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,61 @@
+"""The C ABI library and the drop-in static library: they load, export every
+symbol the headers declare, and keep the reference's layouts.  CPU only (no
+call that needs a GPU)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+import halloc_b200 as H
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions(header: str) -> list:
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|double|uint32_t|void)\s+\**(ha_\w+)\s*\(",
+                                 text, flags=re.M)))
+
+
+def test_header_declares_abi():
+    names = declared_functions("halloc_c.h")
+    assert "ha_init_c" in names and "ha_trace_c" in names and len(names) >= 16
+
+
+def test_shared_library_exports_every_declared_symbol():
+    lib = H.load()
+    missing = [n for n in declared_functions("halloc_c.h") if not hasattr(lib, n)]
+    assert missing == []
+
+
+def test_static_library_keeps_reference_symbols():
+    """A halloc program links against libhalloc.a unchanged: the device and
+    host entry points carry the reference's C++ mangled names."""
+    a = os.path.join(ROOT, "halloc_b200", "libhalloc.a")
+    out = subprocess.run(["nm", a], capture_output=True, text=True, check=True).stdout
+    for sym in ("_Z8hamallocm", "_Z6hafreePv", "_Z7ha_init13halloc_opts_t",
+                "_Z11ha_shutdownv", "_Z10ha_extfragb"):
+        assert re.search(rf"\bT {sym}\b", out), sym
+
+
+def test_options_layout_matches_halloc_opts_t():
+    """x86-64 layout of halloc_opts_t: size_t + 4 doubles + int, 48 bytes."""
+    assert ctypes.sizeof(H._COpts) == 48
+    assert H._COpts.sb_sz_sh.offset == 40
+    d = H.HallocOpts()
+    assert (d.memory, d.halloc_fraction, d.busy_fraction, d.roomy_fraction,
+            d.sparse_fraction, d.sb_sz_sh) == (512 << 20, 0.75, 0.835, 0.6, 0.012, 22)
+
+
+def test_stats_layout():
+    assert ctypes.sizeof(H._CStats) == 5 * 8 + 8 * 4 + 32 * 4
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    monkeypatch.setattr(H, "SO_PATH", str(tmp_path / "absent.so"))
+    monkeypatch.setattr(H, "_lib", None)
+    with pytest.raises(H.HallocError):
+        H.load()

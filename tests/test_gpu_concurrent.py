@@ -1,0 +1,203 @@
+"""Concurrent use: many threads allocating and freeing at once.  Checks the
+reference's own invariants (non-NULL while space is left, no overlap,
+halloc tst/common/common.cu:412-529), the ones it lacked (alignment, pool
+range, payload checksum), and that after quiescence the device's per-slab
+used-chunk counts, bit arrays and size nibbles equal what the host model
+derives from the live blocks."""
+import numpy as np
+import pytest
+
+from tests.helpers import (allocator, check_blocks, expected_slab_state,
+                           nibbles_to_chunk_layout, plain_checksum)
+
+pytestmark = pytest.mark.gpu
+
+SMALL = [16, 24, 32, 48, 64, 96, 128, 192, 256]
+
+
+def malloc_batch(torch, H, sizes: np.ndarray, nthreads: int, nallocs: int):
+    d_sizes = torch.tensor(sizes.astype(np.int32), device="cuda")
+    ptrs = torch.zeros(nthreads * nallocs, dtype=torch.int64, device="cuda")
+    H.malloc_batch(d_sizes, nthreads, nallocs, ptrs, tag=True)
+    torch.cuda.synchronize()
+    return ptrs
+
+
+def assert_state_matches_live(H, ptrs: np.ndarray, sizes: np.ndarray):
+    dump = H.dump_state()
+    counts, bits, nib = expected_slab_state(ptrs, sizes, dump["pool_base"], dump["sb_sz"],
+                                            dump["nsbs"])
+    assert np.array_equal(dump["counters"] >> 12, counts), "per-slab used-chunk counts"
+    assert np.array_equal(dump["bits"], bits), "bit arrays"
+    assert np.array_equal(nibbles_to_chunk_layout(dump["nibbles"], dump["chunk_enc"]), nib)
+    return dump
+
+
+def assert_empty(H):
+    dump = H.dump_state()
+    assert (dump["counters"] >> 12 == 0).all()
+    assert not dump["bits"].any() and not dump["nibbles"].any()
+
+
+def test_plain_config_blocks(torch_cuda):
+    """256 x 128 threads, 4 blocks of 16 B each, held at once."""
+    torch = torch_cuda
+    n, k = 32768, 4
+    sizes = np.full(n * k, 16, np.int64)
+    with allocator(memory=512 << 20) as H:
+        st = H.stats()
+        ptrs = malloc_batch(torch, H, sizes, n, k)
+        p = ptrs.cpu().numpy()
+        check_blocks(p, sizes, st["pool_base"], st["pool_bytes"])
+        assert_state_matches_live(H, p, sizes)
+        H.free_batch(ptrs, n, k)
+        torch.cuda.synchronize()
+        assert_empty(H)
+        assert H.status() == 0
+
+
+def test_mixed_sizes_1m_blocks(torch_cuda):
+    """262144 threads x 4 blocks drawn uniformly from 16..256 B (seeded)."""
+    torch = torch_cuda
+    n, k = 262144, 4
+    rng = np.random.default_rng(7)
+    sizes = rng.choice(SMALL, n * k)
+    with allocator(memory=1 << 30) as H:
+        st = H.stats()
+        ptrs = malloc_batch(torch, H, sizes, n, k)
+        p = ptrs.cpu().numpy()
+        check_blocks(p, sizes, st["pool_base"], st["pool_bytes"])
+        assert_state_matches_live(H, p, sizes)
+        # free half, check again, free the rest
+        half = torch.tensor(np.where(np.arange(n * k) % 2 == 0, p, 0), device="cuda")
+        H.free_batch(half, n, k)
+        torch.cuda.synchronize()
+        rest = np.where(np.arange(n * k) % 2 == 1, p, 0)
+        assert_state_matches_live(H, rest, sizes)
+        H.free_batch(torch.tensor(rest, device="cuda"), n, k)
+        torch.cuda.synchronize()
+        assert_empty(H)
+        assert H.status() == 0
+
+
+def test_large_blocks_go_to_cuda_heap(torch_cuda):
+    torch = torch_cuda
+    n, k = 4096, 2
+    rng = np.random.default_rng(8)
+    sizes = rng.choice([16, 100, 3072, 3073, 4096, 20000], n * k)
+    with allocator(memory=512 << 20) as H:
+        st = H.stats()
+        ptrs = malloc_batch(torch, H, sizes, n, k)
+        p = ptrs.cpu().numpy()
+        check_blocks(p, sizes, st["pool_base"], st["pool_bytes"])
+        assert_state_matches_live(H, p, sizes)
+        H.free_batch(ptrs, n, k)
+        torch.cuda.synchronize()
+        assert_empty(H)
+        assert H.status() == 0
+
+
+def test_exhaustion_returns_null_and_recovers(torch_cuda):
+    """A 32-slab pool asked for twice its size: some requests get NULL, the
+    blocks handed out are still valid, and after freeing everything the same
+    request succeeds again."""
+    torch = torch_cuda
+    n = 65536
+    sizes = np.full(n, 1024, np.int64)
+    with allocator(memory=64 << 20, halloc_fraction=0.5, sb_sz_sh=20) as H:
+        st = H.stats()
+        ptrs = malloc_batch(torch, H, sizes, n, 1)
+        p = ptrs.cpu().numpy()
+        r = check_blocks(p, sizes, st["pool_base"], st["pool_bytes"], allow_null=True)
+        assert r["nnull"] > 0 and r["n"] > 20000
+        assert H.stats()["n_null"] >= r["nnull"]
+        assert_state_matches_live(H, p, sizes)
+        H.free_batch(ptrs, n, 1)
+        torch.cuda.synchronize()
+        assert_empty(H)
+        ptrs2 = malloc_batch(torch, H, np.full(20000, 1024, np.int64), 20000, 1)
+        check_blocks(ptrs2.cpu().numpy(), np.full(20000, 1024), st["pool_base"],
+                     st["pool_bytes"])
+        H.free_batch(ptrs2, 20000, 1)
+        torch.cuda.synchronize()
+        assert H.status() == 0
+
+
+def test_freed_slabs_are_reused_across_sizes(torch_cuda):
+    """The reference's freeslabs test (tst/corr/freeslabs/freeslabs.cu:43-70):
+    sizes 16..1024, each allocating 40 % of the memory and freeing it; it only
+    passes if slabs released by one size serve the next."""
+    torch = torch_cuda
+    memory = 512 << 20
+    sizes_swept = []
+    s, step = 16, 8
+    while s <= 1024:
+        sizes_swept.append(s)
+        s += step
+        step = 128 if s >= 256 else 16 if s >= 64 else 8
+    with allocator(memory=memory) as H:
+        st = H.stats()
+        for sz in sizes_swept:
+            n = min(1 << 20, int(0.4 * memory / sz))
+            sizes = np.full(n, sz, np.int64)
+            ptrs = malloc_batch(torch, H, sizes, n, 1)
+            check_blocks(ptrs.cpu().numpy(), sizes, st["pool_base"], st["pool_bytes"])
+            H.free_batch(ptrs, n, 1)
+            torch.cuda.synchronize()
+        assert_empty(H)
+        assert H.stats()["free_slabs"] >= st["nsbs"] - 2 * 16
+        assert H.status() == 0
+
+
+@pytest.mark.parametrize("nallocs,niters", [(1, 10), (4, 3)])
+def test_throughput_loop_checksum(torch_cuda, nallocs, niters):
+    """The private-throughput loop writes {t^0..t^3} into every block and
+    reads it back: any overlap between live blocks breaks the checksum."""
+    torch = torch_cuda
+    n = 32768
+    with allocator(memory=512 << 20) as H:
+        out = torch.zeros(2, dtype=torch.int64, device="cuda")
+        H.throughput(out, n, nbytes=16, block=128, nallocs=nallocs, niters=niters)
+        torch.cuda.synchronize()
+        cs, nfail = out.cpu().tolist()
+        assert nfail == 0
+        assert cs == plain_checksum(n, nallocs * niters)
+        st = H.stats()
+        assert st["used_chunks"] == 0 and st["status"] == 0
+
+
+def test_throughput_loop_mixed_sizes_host_api(torch_cuda):
+    torch = torch_cuda
+    n = 65536
+    rng = np.random.default_rng(9)
+    h_sizes = rng.choice(SMALL + [512, 3072], n).astype(np.uint32)
+    with allocator(memory=1 << 30) as H:
+        d_sizes = torch.zeros(n, dtype=torch.int32, device="cuda")
+        d_out = torch.zeros(2, dtype=torch.int64, device="cuda")
+        h_out = np.zeros(2, np.uint64)
+        H.throughput_host(h_out, d_out, n, nallocs=2, niters=4, h_sizes=h_sizes,
+                          d_sizes=d_sizes)
+        assert int(h_out[1]) == 0
+        assert int(h_out[0]) == plain_checksum(n, 8)
+        assert H.stats()["used_chunks"] == 0
+
+
+def test_cuda_malloc_comparator_checksum(torch_cuda):
+    torch = torch_cuda
+    n = 4096
+    with allocator(memory=512 << 20) as H:
+        out = torch.zeros(2, dtype=torch.int64, device="cuda")
+        H.cuda_throughput(out, n, nbytes=16, niters=2)
+        torch.cuda.synchronize()
+        cs, nfail = out.cpu().tolist()
+        assert nfail == 0 and cs == plain_checksum(n, 2)
+
+
+def test_stats_and_extfrag(torch_cuda):
+    with allocator(memory=512 << 20) as H:
+        st = H.stats()
+        assert st["nsbs"] == 96 and st["sb_sz"] == 4 << 20
+        assert st["free_slabs"] == 96 and st["used_chunks"] == 0
+        assert st["pool_base"] % (4 << 20) == 0
+        f = H.extfrag(False)
+        assert 0.0 <= f <= 1.0
