@@ -28,6 +28,25 @@ int launch_status() {
 
 uint32_t blocks_for(uint64_t n, uint32_t block) { return (uint32_t)((n + block - 1) / block); }
 
+// 16 payload bytes at a block start.  Blocks of the 24-byte chunk classes
+// start on 8-byte boundaries only, so the 16-byte vector access is used when
+// the block is 16-byte aligned and two 8-byte accesses otherwise.
+__device__ __forceinline__ void store16(void *p, uint4 v) {
+  if (((uintptr_t)p & 15u) == 0) {
+    *reinterpret_cast<uint4 *>(p) = v;
+  } else {
+    uint2 *q = reinterpret_cast<uint2 *>(p);
+    q[0] = make_uint2(v.x, v.y);
+    q[1] = make_uint2(v.z, v.w);
+  }
+}
+__device__ __forceinline__ uint4 load16(const void *p) {
+  if (((uintptr_t)p & 15u) == 0) return __ldcg(reinterpret_cast<const uint4 *>(p));
+  const uint2 a = __ldcg(reinterpret_cast<const uint2 *>(p));
+  const uint2 b = __ldcg(reinterpret_cast<const uint2 *>(p) + 1);
+  return make_uint4(a.x, a.y, b.x, b.y);
+}
+
 // block-wide sum of two counters, one atomic per block
 __device__ __forceinline__ void block_add2(unsigned long long a, unsigned long long b,
                                            unsigned long long *out) {
@@ -97,14 +116,14 @@ __global__ void ha_throughput_k(const uint32_t *sizes, uint32_t nbytes, uint32_t
         void *p = kCudaHeap ? malloc(sz) : hamalloc(sz);
         ps[a] = p;
         if (p)
-          *reinterpret_cast<uint4 *>(p) = word;
+          store16(p, word);
         else
           nfail++;
       }
       for (uint32_t a = 0; a < nallocs; a++) {
         void *p = ps[a];
         if (!p) continue;
-        const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(p));
+        const uint4 v = load16(p);
         sum += (unsigned long long)v.x + v.y + v.z + v.w;
         if (kCudaHeap)
           free(p);
