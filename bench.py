@@ -34,6 +34,9 @@ NTHREADS, BLOCK, NITERS, NALLOCS, NBYTES = 32768, 128, 10, 1, 16
 POOL = 512 << 20
 PAIRS_PER_STEP = NTHREADS * NITERS * NALLOCS
 ATOMICS_PER_PAIR = 2  # one bit-array reservation + one release
+# DRAM bytes (read + write) of one launch of the plain kernel, from an ncu
+# capture of the current build (the bench cannot read DRAM counters itself)
+PLAIN_DRAM_BYTES_PER_LAUNCH = 412672
 METRIC = "16B malloc/free pairs/s"
 WORKLOAD = ("plain: 256 blocks x 128 threads, hamalloc(16) + 16-B write + read-back + hafree, "
             "10 iterations per thread, 512 MiB pool, default halloc_opts_t")
@@ -257,7 +260,64 @@ def run_ours(args, rank, world, local_rank):
                               "failed_allocs": cnf,
                               "heap_bytes": H.stats()["cuda_heap_bytes"]}
     H.shutdown()
+    if rank == 0 and not args.only_gpu and not args.skip_phase:
+        res["phase"] = run_phase(torch, H, 3, hbm_peak())
     return res
+
+
+PHASE_SIZES = [16, 24, 32, 48, 64, 96, 128, 192, 256]
+PHASE_THREADS, PHASE_SLOTS, PHASE_PERIODS, PHASE_POOL = 1 << 20, 4, 5, 1 << 30
+THR95 = int(0.95 * 2**32)
+
+
+def run_phase(torch, H, reps: int, hbm_peak_gbs: float | None) -> dict:
+    """Mixed-size phase workload: 1,048,576 threads x 4 slots, 1 GiB pool,
+    sizes uniform over 16..256 B, 5 periods of (allocation rounds with p=0.95
+    until 91 % of the slots are filled; a free round with p=0.95), then the
+    rest freed; every block written with a hashed pattern and read back
+    before it is freed."""
+    H.init(H.HallocOpts(memory=PHASE_POOL))
+    stream = torch.cuda.current_stream()
+    H.l2_persist(stream)
+    n = PHASE_THREADS
+    size_set = torch.tensor(PHASE_SIZES, dtype=torch.int32, device="cuda")
+    slots = torch.zeros(PHASE_SLOTS * n, dtype=torch.int64, device="cuda")
+    slot_sz = torch.zeros(PHASE_SLOTS * n, dtype=torch.int32, device="cuda")
+    acc = torch.zeros(6, dtype=torch.int64, device="cuda")
+    target = int(0.91 * PHASE_SLOTS * n)
+    runs = []
+    for r in range(reps + 1):  # the first run is warm-up
+        res = H.phase_run(n, PHASE_SLOTS, 0x5EED + r, PHASE_PERIODS, THR95, THR95, target,
+                          size_set, len(PHASE_SIZES), slots, slot_sz, acc, stream=stream)
+        if r:
+            runs.append(res)
+    ok = all(x["failed"] == 0 and x["written_sum"] == x["read_sum"] and
+             x["mallocs"] == x["frees"] for x in runs) and H.status() == 0
+    H.shutdown()
+    ms = sum(x["kernel_ms"] for x in runs)
+    pairs = sum(x["mallocs"] for x in runs)
+    mean = sum(PHASE_SIZES) / len(PHASE_SIZES)
+    gbs = 2 * pairs * mean / (ms * 1e-3) / 1e9
+    out = {"metric": "mixed-size malloc/free pairs/s", "value": pairs / (ms * 1e-3),
+           "unit": "pairs/s", "runs": reps, "ms_per_run": ms / reps,
+           "pairs_per_run": pairs // reps, "rounds_per_run": runs[0]["alloc_rounds"] +
+           runs[0]["free_rounds"], "ok": ok,
+           "config": "1,048,576 threads x 4 slots, 1 GiB pool, sizes uniform "
+                     f"{PHASE_SIZES}, 5 periods (p=0.95 alloc to 91 % slot occupancy, "
+                     "p=0.95 free), hashed payload written and checksummed before free",
+           "payload": {"achieved_gbs": gbs, "bytes_per_pair": 2 * mean,
+                       "note": "written + read once; expected mean block size"}}
+    if hbm_peak_gbs:
+        out["payload"]["frac_of_hbm"] = gbs / hbm_peak_gbs
+    return out
+
+
+def hbm_peak() -> float | None:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return None
 
 
 def cpu_sample(kind: str, seconds: float) -> dict:
@@ -323,7 +383,11 @@ def main_ours(args):
                     "d2h_bytes_per_step": 16,
                     "how": "ha_throughput_host_c from pinned host memory, wall clock"},
             "roofline": {"bound": "l2_atomic", "achieved": achieved / 1e9, "peak": peak / 1e9,
-                         "unit": "Gatomic/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "Gatomic/s", "frac": achieved / peak,
+                         "traffic": PLAIN_DRAM_BYTES_PER_LAUNCH,
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of "
+                                           "one ncu capture of ha_throughput_k (bytes per "
+                                           "launch; profiles/ha_throughput_k_plain.md)",
                          "peak_source": "measured live: distinct-address u32 atomicOr, "
                                         f"{res['peak']}",
                          "algorithmic_atomics_per_pair": ATOMICS_PER_PAIR},
@@ -332,6 +396,7 @@ def main_ours(args):
             "cuda_malloc_baseline": res.get("cuda_malloc"),
             "vs_cuda_malloc": value / world / res["cuda_malloc"]["value"]
             if res.get("cuda_malloc") else None,
+            "phase": res.get("phase"),
             "gpu_launches": args.steps,
             "clocks": res["clocks"],
         }
@@ -382,6 +447,7 @@ def main():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
+    p.add_argument("--skip-phase", action="store_true", help="skip the mixed-size phase leg")
     p.add_argument("--only-gpu", action="store_true",
                    help="skip the CPU and CUDA-malloc legs (profiling runs)")
     args = p.parse_args()

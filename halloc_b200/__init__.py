@@ -23,7 +23,7 @@ import numpy as np
 __all__ = [
     "HallocError", "HallocOpts", "init", "shutdown", "extfrag", "stats", "status",
     "clear_status", "set_wait_limit", "dump_state", "l2_persist", "malloc_batch",
-    "free_batch", "throughput", "throughput_host", "cuda_throughput", "trace",
+    "free_batch", "phase_round", "phase_run", "throughput", "throughput_host", "cuda_throughput", "trace",
     "atomic_peak", "debug_set_head_lock", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
 ]
 
@@ -75,6 +75,12 @@ class _CStats(ctypes.Structure):
                 ("cached", ctypes.c_uint32 * 16)]
 
 
+class _CPhaseResult(ctypes.Structure):
+    _fields_ = [("alloc_rounds", ctypes.c_uint32), ("free_rounds", ctypes.c_uint32),
+                ("kernel_ms", ctypes.c_double), ("filled", ctypes.c_uint64),
+                ("acc", ctypes.c_uint64 * 6)]
+
+
 class _CDump(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in (
         "tickets", "heads", "cached", "size_infos", "counters", "size_id", "chunk_id",
@@ -99,6 +105,10 @@ _SIGS = {
     "ha_throughput_host_c": (_int, [_vp, _vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp, _vp]),
     "ha_cuda_throughput_c": (_int, [_vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp]),
     "ha_trace_c": (_int, [_vp, _i64, _vp, _vp]),
+    "ha_phase_round_c": (_int, [_int, _u32, _u32, _u32, _u32, _u32, _vp, _u32, _vp, _vp, _vp,
+                                _vp]),
+    "ha_phase_run_c": (_int, [_u32, _u32, _u32, _u32, _u32, _u32, ctypes.c_uint64, _u32, _vp,
+                              _u32, _vp, _vp, _vp, ctypes.POINTER(_CPhaseResult), _vp]),
     "ha_atomic_peak_c": (_int, [_vp, _u32, _u32, _u32, _int, _vp]),
 }
 
@@ -261,6 +271,34 @@ def throughput_host(h_out: np.ndarray, d_out, nthreads: int, nbytes: int = 16,
     _check(load().ha_throughput_host_c(_addr(h_sizes), _addr(d_sizes), nbytes, nthreads,
                                        block, nallocs, niters, _addr(d_out), _addr(h_out),
                                        _stream(stream)), "ha_throughput_host_c")
+
+
+def phase_round(kind: int, nthreads: int, nslots: int, seed: int, round_id: int, thr: int,
+                slots, slot_sz, acc, size_set=None, nsizes: int = 0, stream=None) -> None:
+    """One allocation (kind 0) or free (kind 1) round of the phase workload."""
+    _check(load().ha_phase_round_c(kind, nthreads, nslots, seed, round_id, thr,
+                                   _addr(size_set), nsizes, _addr(slots), _addr(slot_sz),
+                                   _addr(acc), _stream(stream)), "ha_phase_round_c")
+
+
+PHASE_ACC = ("filled", "failed", "written_sum", "read_sum", "mallocs", "frees")
+
+
+def phase_run(nthreads: int, nslots: int, seed: int, periods: int, thr_alloc: int,
+              thr_free: int, target_filled: int, size_set, nsizes: int, slots, slot_sz, acc,
+              max_rounds: int = 64, stream=None) -> dict:
+    """The whole phase workload (ha_phase_run_c); device buffers: size_set
+    (nsizes u32), slots (nslots*nthreads pointers, all NULL), slot_sz
+    (nslots*nthreads u32), acc (6 u64)."""
+    r = _CPhaseResult()
+    _check(load().ha_phase_run_c(nthreads, nslots, seed, periods, thr_alloc, thr_free,
+                                 target_filled, max_rounds, _addr(size_set), nsizes,
+                                 _addr(slots), _addr(slot_sz), _addr(acc), ctypes.byref(r),
+                                 _stream(stream)), "ha_phase_run_c")
+    out = {"alloc_rounds": r.alloc_rounds, "free_rounds": r.free_rounds,
+           "kernel_ms": r.kernel_ms, "filled": r.filled}
+    out.update(dict(zip(PHASE_ACC, list(r.acc))))
+    return out
 
 
 def trace(ops, n: int, out, stream=None) -> None:

@@ -31,7 +31,11 @@ CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler", "
 
 HEADERS = [os.path.join(CSRC, f) for f in ("ha_core.cuh", "ha_types.h")] + [
     os.path.join(INCLUDE, f) for f in ("halloc.h", "halloc_c.h")]
-SOURCES = ["halloc.cu", "ha_kernels.cu"]
+# The allocator's device functions are capped at 64 registers: every kernel
+# that calls hamalloc/hafree inherits the callee's register count at device
+# link time, so this bounds the occupancy cost for user kernels (the
+# reference built with the same cap).
+SOURCES = {"halloc.cu": ["-maxrregcount=64"], "ha_kernels.cu": []}
 
 
 def nvcc() -> str:
@@ -62,12 +66,12 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     cc = nvcc()
     objs = []
-    for src in SOURCES:
+    for src, flags in SOURCES.items():
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         if _stale(o, [s, __file__] + HEADERS) or ptxas_info:
             extra = ["-Xptxas", "-v"] if ptxas_info else []
-            _run([cc] + CUFLAGS + extra + ["-c", s, "-o", o], verbose)
+            _run([cc] + CUFLAGS + flags + extra + ["-c", s, "-o", o], verbose)
         objs.append(o)
     halloc_o = objs[0]
     if _stale(LIB_A, [halloc_o]):

@@ -34,6 +34,8 @@ namespace ha {
 // ---------------------------------------------------------------------------
 extern __constant__ Config c_cfg;
 extern __device__ Class g_cls[kNSizes];
+// fastmod magics per size class: nchunks (x, y = low, high word), hash step (z, w)
+extern __device__ uint4 g_mod[kNSizes];
 extern __device__ State g_st;
 
 // ---------------------------------------------------------------------------
@@ -56,7 +58,7 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 }
 __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p) {
   uint32_t v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
   return v;
 }
 __device__ __forceinline__ void st_relaxed(uint32_t *p, uint32_t v) {
@@ -68,29 +70,29 @@ __device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
 __device__ __forceinline__ uint32_t atom_add(uint32_t *p, uint32_t v) {
   uint32_t o;
   asm volatile("atom.relaxed.gpu.global.add.u32 %0, [%1], %2;"
-               : "=r"(o) : "l"(p), "r"(v) : "memory");
+               : "=r"(o) : "l"(p), "r"(v));
   return o;
 }
 __device__ __forceinline__ uint32_t atom_or(uint32_t *p, uint32_t v) {
   uint32_t o;
   asm volatile("atom.relaxed.gpu.global.or.b32 %0, [%1], %2;"
-               : "=r"(o) : "l"(p), "r"(v) : "memory");
+               : "=r"(o) : "l"(p), "r"(v));
   return o;
 }
 __device__ __forceinline__ uint32_t atom_and(uint32_t *p, uint32_t v) {
   uint32_t o;
   asm volatile("atom.relaxed.gpu.global.and.b32 %0, [%1], %2;"
-               : "=r"(o) : "l"(p), "r"(v) : "memory");
+               : "=r"(o) : "l"(p), "r"(v));
   return o;
 }
 __device__ __forceinline__ void red_add(uint32_t *p, uint32_t v) {
-  asm volatile("red.relaxed.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+  asm volatile("red.relaxed.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v));
 }
 __device__ __forceinline__ void red_or(uint32_t *p, uint32_t v) {
-  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v));
 }
 __device__ __forceinline__ void red_and(uint32_t *p, uint32_t v) {
-  asm volatile("red.relaxed.gpu.global.and.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+  asm volatile("red.relaxed.gpu.global.and.b32 [%0], %1;" ::"l"(p), "r"(v));
 }
 __device__ __forceinline__ void fence_acq_rel() {
   asm volatile("fence.acq_rel.gpu;" ::: "memory");
@@ -490,93 +492,111 @@ __device__ __noinline__ uint32_t replace_head(uint32_t sid) {
 // allocation
 // ---------------------------------------------------------------------------
 
+// x mod d from m = floor((2^64 - 1) / d) + 1, exact for every 32-bit x and d
+// (Lemire, Kaser, Kurz: "Faster remainder by direct computation", 2019).
+__device__ __forceinline__ uint32_t fastmod(uint32_t x, uint64_t m, uint32_t d) {
+  return (uint32_t)__umul64hi(m * x, d);
+}
+__device__ __forceinline__ uint64_t mod_magic(uint32_t lo, uint32_t hi) {
+  return ((uint64_t)hi << 32) | lo;
+}
+
 // first probe position of a ticket: tickets_per_slot consecutive tickets
 // share a slot, slots are kHashFreq blocks apart, 32-bit wraparound
 // (halloc src/halloc.cu:107-122)
-__device__ __forceinline__ uint32_t first_probe(const Class &c, uint32_t sid, uint32_t t) {
-  uint32_t low = tickets_per_slot(sid) - 1;
-  uint32_t spread = (t & ~low) * kHashFreq + (t & low);
-  return spread * c.ncib % c.nchunks;
+__device__ __forceinline__ uint32_t first_probe(uint32_t sid, uint32_t ticket, uint32_t ncib,
+                                                uint64_t mn, uint32_t nchunks) {
+  const uint32_t low = tickets_per_slot(sid) - 1;
+  const uint32_t spread = (ticket & ~low) * kHashFreq + (ticket & low);
+  return fastmod(spread * ncib, mn, nchunks);
 }
 
-// Small-block allocation for every lane of the calling warp that is active
-// here; lanes may ask for different sizes.  (halloc src/halloc.cu:125-182
-// and src/slab.cuh:453-535, with the warp protocol rebuilt on explicit
-// masks.)
-__device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
-  const uint32_t warp = __activemask();
+// probe position after try number `round` failed (halloc
+// src/slab.cuh:492-495): step ((round+1) * 64 * ncib) mod hash_step,
+// position (first + (round+1) * step) mod nchunks
+__device__ __forceinline__ uint32_t next_probe(uint32_t first, uint32_t round, uint32_t ncib,
+                                               uint32_t nchunks, uint64_t mn, uint32_t hstep,
+                                               uint64_t mh) {
+  const uint32_t k = round + 1;
+  const uint32_t step = fastmod(k * kStepScale * ncib, mh, hstep);
+  return fastmod(first + k * step, mn, nchunks);
+}
+
+// Continues the reference's probe sequence in slab sb (halloc
+// src/slab.cuh:469-498): tries `pos` as try number `round`, then the next
+// positions, until a block is reserved (true), the slab count reads busy at
+// an odd try, or the 32-try round ends (false).  Per lane, no warp ops.
+__device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t mn, uint64_t mh,
+                                           uint32_t first, uint32_t block, uint32_t &pos,
+                                           uint32_t &round) {
+  uint32_t *bits = bits_of(sb);
+  for (;;) {
+    const uint32_t mask = block << (pos & 31);
+    const uint32_t old = atom_or(&bits[pos >> 5], mask);
+    if (!(old & mask)) return true;
+    if (~old & mask) red_and(&bits[pos >> 5], ~mask | (old & mask));
+    if (round % kCountCheck == kCountCheck - 1 && used_of(sb) >= c.busy) return false;
+    pos = next_probe(first, round, c.ncib, c.nchunks, mn, c.hash_step, mh);
+    if (++round % kTriesPerRound >= kTriesPerRound - 1) return false;
+  }
+}
+
+// Counts the blocks just reserved by the lanes of rmask, one atomic per slab
+// (halloc src/slab.cuh:122-155).  Called by exactly the lanes of rmask.
+// Returns false, after undoing this lane's reservation, when the slab no
+// longer has the caller's chunk size; otherwise *crossed tells whether the
+// count crossed the busy threshold.
+__device__ __forceinline__ bool commit(uint32_t rmask, uint32_t sb, uint32_t ncib,
+                                       uint32_t cid, uint32_t busy, uint32_t pos,
+                                       uint32_t block, bool &crossed) {
+  const uint32_t grp = __match_any_sync(rmask, sb);
+  const uint32_t total = __reduce_add_sync(grp, ncib);
+  const uint32_t lead = __ffs(grp) - 1;
+  uint32_t before = 0;
+  if (lane_id() == lead) before = atom_add(ctr_of(sb), total << kCntShift);
+  before = __shfl_sync(grp, before, lead);
+  const bool ok = ((before >> kChunkShift) & kChunkField) == cid;
+  const uint32_t n0 = before >> kCntShift;
+  crossed = n0 + total >= busy && n0 < busy;
+  const uint32_t cmask = __ballot_sync(rmask, !ok);
+  if (!ok) {
+    // the slab changed chunk size under us: give the block back
+    red_and(&bits_of(sb)[pos >> 5], ~(block << (pos & 31)));
+    count_down(cmask, sb, ncib);
+  }
+  return ok;
+}
+
+__device__ __forceinline__ void *publish(uint32_t sb, uint32_t pos, uint32_t enc,
+                                         uint32_t ncib) {
+  const uint32_t off = chunk_mul(pos, enc);
+  red_or(&nibs_of(sb)[off >> 7], ncib << ((off >> 2) & 28));
+  return slab_ptr(sb) + off;
+}
+
+// per-lane state handed from the fast attempt to the slow path
+constexpr uint32_t kWant = 1;      // no block yet
+constexpr uint32_t kNeedHead = 2;  // ask for a new head slab
+constexpr uint32_t kMidRound = 4;  // continue the current probe call at pos
+
+// The rest of halloc's allocation loop (src/halloc.cu:145-179 with
+// src/slab.cuh:453-535), for the whole warp `warp`: new head slabs for the
+// lanes that need one (one lane per size at a time), then further probe
+// calls for lanes still without a block.  Every lane of `warp` calls it.
+__device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t nbytes, uint32_t ticket,
+                                          uint32_t sb, uint32_t pos, uint32_t round,
+                                          uint32_t flags, void *p) {
   const uint32_t me = lane_id();
   const uint32_t sid = size_class(nbytes);
   const Class c = load_class(sid);
-  uint32_t sb = ld_relaxed(&g_st.head[sid]);
-
-  // ticket: consecutive values for lanes of one size, in lane order
-  uint32_t ticket;
-  {
-    uint32_t grp = __match_any_sync(warp, sid);
-    uint32_t lead = __ffs(grp) - 1, base = 0;
-    if (me == lead) base = atom_add(&g_st.ticket[sid * kTicketStride], __popc(grp));
-    base = __shfl_sync(grp, base, lead);
-    ticket = base + __popc(grp & lanemask_lt());
-  }
-  const uint32_t first = first_probe(c, sid, ticket);
+  const uint4 mm = __ldg(&g_mod[sid]);
+  const uint64_t mn = mod_magic(mm.x, mm.y), mh = mod_magic(mm.z, mm.w);
+  const uint32_t first = first_probe(sid, ticket, c.ncib, mn, c.nchunks);
   const uint32_t block = (1u << c.ncib) - 1u;
-
-  void *p = nullptr;
-  bool want = true;
-  uint32_t round = 0, rounds_total = 0;
-  do {
-    bool need_head = false;
-    const uint32_t want_mask = __ballot_sync(warp, want);
-    if (want) {
-      // -- probe the head slab (per lane, no warp ops inside) --------------
-      bool reserved = false;
-      uint32_t pos = first;
-      if (sb == kNone) {
-        need_head = true;
-      } else {
-        uint32_t *bits = bits_of(sb);
-        do {
-          uint32_t mask = block << (pos & 31);
-          uint32_t old = atom_or(&bits[pos >> 5], mask);
-          if (!(old & mask)) {
-            reserved = true;
-            break;
-          }
-          if (~old & mask) red_and(&bits[pos >> 5], ~mask | (old & mask));
-          if (round % kCountCheck == kCountCheck - 1 && used_of(sb) >= c.busy) break;
-          uint32_t k = round + 1;
-          uint32_t step = k * kStepScale * c.ncib % c.hash_step;
-          pos = (first + k * step) % c.nchunks;
-        } while (++round % kTriesPerRound < kTriesPerRound - 1);
-        if (!reserved) need_head = true;
-      }
-      // -- count the reservation, aggregated per slab ----------------------
-      const uint32_t rmask = __ballot_sync(want_mask, reserved);
-      if (reserved) {
-        uint32_t grp = __match_any_sync(rmask, sb);
-        uint32_t total = __reduce_add_sync(grp, c.ncib);
-        uint32_t lead = __ffs(grp) - 1, before = 0;
-        if (me == lead) before = atom_add(ctr_of(sb), total << kCntShift);
-        before = __shfl_sync(grp, before, lead);
-        const bool ok = ((before >> kChunkShift) & kChunkField) == c.chunk_id;
-        const uint32_t n0 = before >> kCntShift;
-        const uint32_t cmask = __ballot_sync(rmask, !ok);
-        if (!ok) {
-          // the slab changed chunk size under us: give the block back
-          red_and(&bits_of(sb)[pos >> 5], ~(block << (pos & 31)));
-          count_down(cmask, sb, c.ncib);
-          need_head = true;
-        } else {
-          if (n0 + total >= c.busy && n0 < c.busy) need_head = true;
-          uint32_t off = chunk_mul(pos, c.chunk_enc);
-          red_or(&nibs_of(sb)[off >> 7], c.ncib << ((off >> 2) & 28));
-          p = slab_ptr(sb) + off;
-          want = false;
-        }
-      }
-    }
-    // -- new head slabs, one lane per size at a time ------------------------
+  bool want = flags & kWant, need_head = flags & kNeedHead, mid = flags & kMidRound;
+  uint32_t rounds = 0;
+  for (;;) {
+    // -- new head slabs -------------------------------------------------------
     uint32_t nmask = __ballot_sync(warp, need_head);
     while (nmask) {
       const uint32_t lead = __ffs(nmask) - 1;
@@ -591,12 +611,98 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
       }
       nmask = __ballot_sync(warp, need_head);
     }
-    if (want && ++rounds_total > kMaxRounds) {
+    if (want && ++rounds > kMaxRounds) {
       raise_status(HA_ST_LIVELOCK);
       want = false;
     }
-  } while (__any_sync(warp, want));
+    const uint32_t want_mask = __ballot_sync(warp, want);
+    if (!want_mask) break;
+    if (want) {
+      bool reserved = false;
+      if (sb == kNone) {
+        need_head = true;
+      } else {
+        if (!mid) pos = first;  // a new probe call starts at the first position
+        reserved = probe_from(sb, c, mn, mh, first, block, pos, round);
+        if (!reserved) need_head = true;
+      }
+      mid = false;
+      const uint32_t rmask = __ballot_sync(want_mask, reserved);
+      if (reserved) {
+        bool crossed;
+        if (commit(rmask, sb, c.ncib, c.chunk_id, c.busy, pos, block, crossed)) {
+          if (crossed) need_head = true;
+          p = publish(sb, pos, c.chunk_enc, c.ncib);
+          want = false;
+        } else {
+          need_head = true;
+        }
+      }
+    }
+  }
   if (!p) red_add(&g_st.n_null, 1);
+  return p;
+}
+
+// Small-block allocation for the lanes of the calling warp that are active
+// here; lanes may ask for different sizes.  Fast path: ticket, one probe in
+// the head slab, one counter atomic per slab, the size nibble.  Everything
+// else (further probes, head replacement, exhaustion) continues in
+// malloc_slow exactly where the reference's loop would.
+// (halloc src/halloc.cu:125-182)
+__device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
+  const uint32_t warp = __activemask();
+  const uint32_t sid = size_class(nbytes);
+  const uint4 ca = __ldg(reinterpret_cast<const uint4 *>(&g_cls[sid]));
+  const uint32_t nchunks = ca.x, enc = ca.y, cid = ca.z, ncib = ca.w;
+  uint32_t sb = ld_relaxed(&g_st.head[sid]);
+
+  // ticket: consecutive values for lanes of one size, in lane order
+  uint32_t ticket;
+  {
+    const uint32_t grp = __match_any_sync(warp, sid);
+    const uint32_t lead = __ffs(grp) - 1;
+    uint32_t base = 0;
+    if (lane_id() == lead) base = atom_add(&g_st.ticket[sid * kTicketStride], __popc(grp));
+    base = __shfl_sync(grp, base, lead);
+    ticket = base + __popc(grp & lanemask_lt());
+  }
+  const uint4 mm = __ldg(&g_mod[sid]);
+  const uint64_t mn = mod_magic(mm.x, mm.y);
+  const uint32_t first = first_probe(sid, ticket, ncib, mn, nchunks);
+  const uint32_t block = (1u << ncib) - 1u;
+
+  uint32_t pos = first, round = 0, flags = kWant;
+  bool reserved = false;
+  if (sb == kNone) {
+    flags |= kNeedHead;
+  } else {
+    const uint32_t mask = block << (pos & 31);
+    uint32_t *w = &bits_of(sb)[pos >> 5];
+    const uint32_t old = atom_or(w, mask);
+    if (!(old & mask)) {
+      reserved = true;
+    } else {
+      if (~old & mask) red_and(w, ~mask | (old & mask));
+      // try 0 failed: no count check at an even try; move to try 1
+      const uint32_t hstep = __ldg(&g_cls[sid].hash_step);
+      pos = next_probe(first, 0, ncib, nchunks, mn, hstep, mod_magic(mm.z, mm.w));
+      round = 1;
+      flags |= kMidRound;
+    }
+  }
+  void *p = nullptr;
+  const uint32_t rmask = __ballot_sync(warp, reserved);
+  if (reserved) {
+    bool crossed;
+    if (commit(rmask, sb, ncib, cid, __ldg(&g_cls[sid].busy), pos, block, crossed)) {
+      p = publish(sb, pos, enc, ncib);
+      flags = crossed ? kNeedHead : 0;
+    } else {
+      flags = kWant | kNeedHead;
+    }
+  }
+  if (__any_sync(warp, flags != 0)) p = malloc_slow(warp, nbytes, ticket, sb, pos, round, flags, p);
   return p;
 }
 
@@ -614,13 +720,19 @@ __device__ __forceinline__ void free_small(uint64_t off) {
   const uint32_t enc = ld_relaxed(&g_st.desc[sb].chunk_enc);
   const uint32_t old = atom_and(nw, ~(15u << sh));
   const uint32_t n = (old >> sh) & 15u;
-  bool valid = n != 0 && enc != 0;
+  const bool valid = n != 0 && enc != 0;
   if (!valid) raise_status(HA_ST_BAD_FREE);
   const uint32_t ichunk = valid ? chunk_div(in, enc) : 0;
   if (valid) red_and(&bits_of(sb)[ichunk >> 5], ~(((1u << n) - 1u) << (ichunk & 31)));
-  const uint32_t active = __activemask();
-  const uint32_t vmask = __ballot_sync(active, valid);
-  if (valid) count_down(vmask, sb, n);
+  const uint32_t vmask = __ballot_sync(__activemask(), valid);
+  if (valid) {
+    const uint32_t grp = __match_any_sync(vmask, sb);
+    const uint32_t total = __reduce_add_sync(grp, n);
+    if (lane_id() == (uint32_t)(__ffs(grp) - 1)) {
+      const uint32_t before = atom_add(ctr_of(sb), 0u - (total << kCntShift));
+      if (!(before & kHeadFlag)) file_after_free(sb, before, total);
+    }
+  }
 }
 
 }  // namespace ha

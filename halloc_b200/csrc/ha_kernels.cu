@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <string.h>
 
 #include "halloc.h"
 #include "halloc_c.h"
@@ -47,10 +48,11 @@ __device__ __forceinline__ uint4 load16(const void *p) {
   return make_uint4(a.x, a.y, b.x, b.y);
 }
 
-// block-wide sum of two counters, one atomic per block
+// block-wide sums of two counters, one atomic each per block
 __device__ __forceinline__ void block_add2(unsigned long long a, unsigned long long b,
-                                           unsigned long long *out) {
+                                           unsigned long long *pa, unsigned long long *pb) {
   __shared__ unsigned long long sa[32], sb[32];
+  __syncthreads();  // a previous call may still be reading sa / sb
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_down_sync(0xffffffffu, a, o);
     b += __shfl_down_sync(0xffffffffu, b, o);
@@ -70,8 +72,8 @@ __device__ __forceinline__ void block_add2(unsigned long long a, unsigned long l
       b += __shfl_down_sync(0xffffffffu, b, o);
     }
     if (lane == 0) {
-      if (a) atomicAdd(&out[0], a);
-      if (b) atomicAdd(&out[1], b);
+      if (a) atomicAdd(pa, a);
+      if (b) atomicAdd(pb, b);
     }
   }
 }
@@ -132,7 +134,103 @@ __global__ void ha_throughput_k(const uint32_t *sizes, uint32_t nbytes, uint32_t
       }
     }
   }
-  block_add2(sum, nfail, out);
+  block_add2(sum, nfail, out, out + 1);
+}
+
+// ---- phase workload ----------------------------------------------------------
+//
+// Every decision (allocate this slot? which size? free it?) and every
+// payload word comes from a counter-based hash of (seed, thread, slot,
+// round), so a host can replay the whole run and predict its checksums
+// whatever the device scheduling was.
+
+// "lowbias32" integer finaliser (C. Wellons, public domain hash prospector)
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+__device__ __forceinline__ uint32_t slot_hash(uint32_t seed, uint32_t i, uint32_t s,
+                                              uint32_t round) {
+  return mix32(((i << 2) | s) ^ (round * 0x9E3779B9u) ^ seed);
+}
+
+// Phase accumulators: [0] slots filled after the round, [1] failed
+// allocations, [2] sum of words written, [3] sum of words read back,
+// [4] allocations, [5] frees.
+//
+// One allocation round: every empty slot of every thread is filled with
+// probability thr / 2^32 by a block of a size drawn from size_set, whose
+// words are written with base, base+1, ...
+__global__ void ha_phase_alloc_k(uint32_t n, uint32_t nslots, uint32_t seed, uint32_t round,
+                                 uint32_t thr, const uint32_t *size_set, uint32_t nsizes,
+                                 void **slots, uint32_t *slot_sz, unsigned long long *acc) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long filled = 0, nfail = 0, wsum = 0, nmal = 0;
+  if (i < n) {
+    for (uint32_t s = 0; s < nslots; s++) {
+      const size_t k = (size_t)s * n + i;
+      void *p = slots[k];
+      if (!p) {
+        const uint32_t h = slot_hash(seed, i, s, round);
+        if (h < thr) {
+          const uint32_t sz = size_set[mix32(h ^ 0xA5A5A5A5u) % nsizes];
+          p = hamalloc(sz);
+          if (p) {
+            const uint32_t base = mix32(h ^ 0x5EED5EEDu);
+            uint2 *q = reinterpret_cast<uint2 *>(p);
+            for (uint32_t w = 0; w < sz / 8; w++) {
+              const uint32_t a = base + 2 * w, b = base + 2 * w + 1;
+              q[w] = make_uint2(a, b);
+              wsum += (unsigned long long)a + b;
+            }
+            slots[k] = p;
+            slot_sz[k] = sz;
+            nmal++;
+          } else {
+            nfail++;
+          }
+        }
+      }
+      if (p) filled++;
+    }
+  }
+  block_add2(filled, nfail, acc, acc + 1);
+  block_add2(wsum, nmal, acc + 2, acc + 4);
+}
+
+// One free round: every live block is read back and freed with
+// probability thr / 2^32 (always when thr is 0xffffffff).
+__global__ void ha_phase_free_k(uint32_t n, uint32_t nslots, uint32_t seed, uint32_t round,
+                                uint32_t thr, void **slots, const uint32_t *slot_sz,
+                                unsigned long long *acc) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long filled = 0, rsum = 0, nfree = 0;
+  if (i < n) {
+    for (uint32_t s = 0; s < nslots; s++) {
+      const size_t k = (size_t)s * n + i;
+      void *p = slots[k];
+      if (!p) continue;
+      if (thr == 0xffffffffu || slot_hash(seed, i, s, round) < thr) {
+        const uint2 *q = reinterpret_cast<const uint2 *>(p);
+        const uint32_t sz = slot_sz[k];
+        for (uint32_t w = 0; w < sz / 8; w++) {
+          const uint2 v = __ldcg(q + w);
+          rsum += (unsigned long long)v.x + v.y;
+        }
+        hafree(p);
+        slots[k] = nullptr;
+        nfree++;
+      } else {
+        filled++;
+      }
+    }
+  }
+  block_add2(filled, rsum, acc, acc + 3);
+  block_add2(nfree, 0, acc + 5, acc + 5);
 }
 
 // serial replay on one thread
@@ -235,6 +333,79 @@ extern "C" int ha_throughput_host_c(const uint32_t *h_sizes, uint32_t *d_sizes,
       cudaStreamSynchronize(s) != cudaSuccess)
     return HA_ECUDA;
   return HA_OK;
+}
+
+extern "C" int ha_phase_round_c(int kind, uint32_t nthreads, uint32_t nslots, uint32_t seed,
+                                uint32_t round, uint32_t thr, const uint32_t *size_set,
+                                uint32_t nsizes, void **slots, uint32_t *slot_sz, uint64_t *acc,
+                                void *stream) {
+  if (!slots || !slot_sz || !acc || nslots == 0 || nslots > kMaxAllocsPerThread ||
+      (kind == 0 && (!size_set || nsizes == 0)) || (kind != 0 && kind != 1))
+    return HA_EINVAL;
+  if (nthreads == 0) return HA_OK;
+  cudaStream_t s = as_stream(stream);
+  if (cudaMemsetAsync(acc, 0, sizeof(uint64_t), s) != cudaSuccess) return HA_ECUDA;
+  unsigned long long *a = reinterpret_cast<unsigned long long *>(acc);
+  const uint32_t grid = blocks_for(nthreads, 128);
+  if (kind == 0)
+    ha_phase_alloc_k<<<grid, 128, 0, s>>>(nthreads, nslots, seed, round, thr, size_set, nsizes,
+                                          slots, slot_sz, a);
+  else
+    ha_phase_free_k<<<grid, 128, 0, s>>>(nthreads, nslots, seed, round, thr, slots, slot_sz, a);
+  return launch_status();
+}
+
+extern "C" int ha_phase_run_c(uint32_t nthreads, uint32_t nslots, uint32_t seed,
+                              uint32_t periods, uint32_t thr_alloc, uint32_t thr_free,
+                              uint64_t target_filled, uint32_t max_rounds,
+                              const uint32_t *size_set, uint32_t nsizes, void **slots,
+                              uint32_t *slot_sz, uint64_t *acc, ha_phase_result_t *res,
+                              void *stream) {
+  if (!res || !acc) return HA_EINVAL;
+  cudaStream_t s = as_stream(stream);
+  memset(res, 0, sizeof(*res));
+  if (cudaMemsetAsync(acc, 0, 6 * sizeof(uint64_t), s) != cudaSuccess) return HA_ECUDA;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return HA_ECUDA;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return HA_ECUDA;
+  }
+  int rc = HA_OK;
+  uint32_t round = 0;
+  auto run = [&](int kind, uint32_t thr) -> int {
+    if (cudaEventRecord(e0, s) != cudaSuccess) return HA_ECUDA;
+    int r = ha_phase_round_c(kind, nthreads, nslots, seed, round++, thr, size_set, nsizes,
+                             slots, slot_sz, acc, stream);
+    if (r) return r;
+    float ms = 0.f;
+    if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      return HA_ECUDA;
+    res->kernel_ms += ms;
+    if (kind == 0)
+      res->alloc_rounds++;
+    else
+      res->free_rounds++;
+    return cudaMemcpy(&res->filled, acc, sizeof(uint64_t), cudaMemcpyDeviceToHost) ==
+                   cudaSuccess
+               ? HA_OK
+               : HA_ECUDA;
+  };
+  for (uint32_t per = 0; per < periods && rc == HA_OK; per++) {
+    for (uint32_t r = 0; r < max_rounds && rc == HA_OK; r++) {
+      rc = run(0, thr_alloc);
+      if (rc == HA_OK && res->filled >= target_filled) break;
+    }
+    if (rc == HA_OK) rc = run(1, thr_free);
+  }
+  if (rc == HA_OK) rc = run(1, 0xffffffffu);  // the rest, as in the reference's free_rest_k
+  if (rc == HA_OK &&
+      cudaMemcpy(res->acc, acc, 6 * sizeof(uint64_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = HA_ECUDA;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
 }
 
 extern "C" int ha_trace_c(const int64_t *ops, int64_t n, int64_t *out, void *stream) {

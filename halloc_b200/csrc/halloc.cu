@@ -26,6 +26,7 @@ static_assert(offsetof(halloc_opts_t, sb_sz_sh) == offsetof(ha_opts_c, sb_sz_sh)
 namespace ha {
 __constant__ Config c_cfg;
 __device__ Class g_cls[kNSizes];
+__device__ uint4 g_mod[kNSizes];
 __device__ State g_st;
 
 // statistics scratch, written by stats_k
@@ -136,6 +137,16 @@ bool build_classes(ha::Class *cls, uint32_t sb_bytes, const ha_opts_c &o) {
   return true;
 }
 
+// fastmod magic of a 32-bit divisor: floor((2^64 - 1) / d) + 1
+uint64_t mod_magic(uint32_t d) { return ~0ull / d + 1; }
+
+void build_magics(const ha::Class *cls, uint4 *mod) {
+  for (uint32_t sid = 0; sid < ha::kNSizes; sid++) {
+    uint64_t mn = mod_magic(cls[sid].nchunks), mh = mod_magic(cls[sid].hash_step);
+    mod[sid] = make_uint4((uint32_t)mn, (uint32_t)(mn >> 32), (uint32_t)mh, (uint32_t)(mh >> 32));
+  }
+}
+
 bool valid_fraction(double f) { return f >= 0.0 && f <= 1.0; }
 
 int shutdown_impl() {
@@ -182,6 +193,8 @@ int init_impl(const ha_opts_c &o) {
 
   ha::Class cls[ha::kNSizes];
   if (!build_classes(cls, sb_bytes, o)) return HA_EINVAL;
+  uint4 mod[ha::kNSizes];
+  build_magics(cls, mod);
 
   // CUDA heap for blocks above 3072 bytes.  The size cannot change once a
   // kernel of this context has used in-kernel malloc; the allocator still
@@ -237,6 +250,7 @@ int init_impl(const ha_opts_c &o) {
     cfg.sum_words = (cfg.set_words + 31) / 32;
     if (cudaMemset(meta, 0, meta_bytes) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_cls, cls, sizeof(cls)) != cudaSuccess ||
+        cudaMemcpyToSymbol(ha::g_mod, mod, sizeof(mod)) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_st, st, sizeof(*st)) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::c_cfg, &cfg, sizeof(cfg)) != cudaSuccess ||
         cudaDeviceSynchronize() != cudaSuccess) {

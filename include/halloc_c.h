@@ -155,6 +155,46 @@ int ha_cuda_throughput_c(const uint32_t *sizes, uint32_t nbytes,
                          uint32_t nthreads, uint32_t block, uint32_t nallocs,
                          uint32_t niters, uint64_t *out, void *stream);
 
+/* One round of the mixed-size phase workload (nthreads threads, nslots
+   block slots each; slots[s*nthreads + i] is NULL when empty, slot_sz its
+   block size).  kind 0 (allocation round): each empty slot is filled with
+   probability thr / 2^32 by hamalloc of a size drawn from size_set[nsizes],
+   and the block's 32-bit words are written base, base+1, ...; kind 1 (free
+   round): each live block is read back and hafree'd with probability
+   thr / 2^32 (always for thr = 0xffffffff).  Decisions, sizes and bases
+   come from a hash of (seed, thread, slot, round).  acc (6 device words):
+   acc[0] is set to the slots filled after the round; acc[1] += failed
+   allocations, acc[2] += sum of words written, acc[3] += sum of words read
+   back, acc[4] += allocations, acc[5] += frees.  Replaces
+   prob_throughput_k / prob_corr_k (halloc
+   tst/perf/phase-throughput/phase-throughput.cu:14-47,
+   tst/corr/prob-checkptr/prob-checkptr.cu:14-45) with an occupancy-driven
+   phase schedule. */
+int ha_phase_round_c(int kind, uint32_t nthreads, uint32_t nslots, uint32_t seed,
+                     uint32_t round, uint32_t thr, const uint32_t *size_set,
+                     uint32_t nsizes, void **slots, uint32_t *slot_sz, uint64_t *acc,
+                     void *stream);
+
+typedef struct ha_phase_result_t {
+  uint32_t alloc_rounds, free_rounds;
+  double kernel_ms;   /* sum of the rounds' kernel times (CUDA events) */
+  uint64_t filled;    /* slots filled after the last round */
+  uint64_t acc[6];    /* final accumulators, as in ha_phase_round_c */
+} ha_phase_result_t;
+
+/* The whole phase workload: `periods` times (allocation rounds until at
+   least target_filled slots are filled, at most max_rounds; one free
+   round), then a round freeing every remaining block.  Round r uses round
+   number r in the hash.  The host loop of the reference's phase-throughput
+   test (halloc tst/perf/phase-throughput/phase-throughput.cu:149-192),
+   driven by occupancy instead of fixed transition probabilities. */
+int ha_phase_run_c(uint32_t nthreads, uint32_t nslots, uint32_t seed,
+                   uint32_t periods, uint32_t thr_alloc, uint32_t thr_free,
+                   uint64_t target_filled, uint32_t max_rounds,
+                   const uint32_t *size_set, uint32_t nsizes, void **slots,
+                   uint32_t *slot_sz, uint64_t *acc, ha_phase_result_t *res,
+                   void *stream);
+
 /* Replays a trace on ONE device thread: op >= 0 is hamalloc(op);
    op < 0 is hafree of the block returned by op index -(op + 1).
    out[i] = the pointer hamalloc returned (0 for NULL) as an integer, and 0

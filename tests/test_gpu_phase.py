@@ -1,0 +1,74 @@
+"""The mixed-size phase workload: 5 periods of occupancy-driven allocation
+rounds and free rounds over 16..256-byte blocks, every block filled with a
+hashed pattern and read back before it is freed.  The device's counts and
+payload sums must equal the host replay of the same hashed decisions, and
+the slab state after an allocation round must equal what the live blocks
+imply."""
+import numpy as np
+import pytest
+
+from oracle.phase import PhaseReplay
+from tests.helpers import allocator, check_blocks, expected_slab_state, nibbles_to_chunk_layout
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [16, 24, 32, 48, 64, 96, 128, 192, 256]
+THR95 = int(0.95 * 2**32)
+
+
+def buffers(torch, n, nslots):
+    size_set = torch.tensor(SIZES, dtype=torch.int32, device="cuda")
+    slots = torch.zeros(nslots * n, dtype=torch.int64, device="cuda")
+    slot_sz = torch.zeros(nslots * n, dtype=torch.int32, device="cuda")
+    acc = torch.zeros(6, dtype=torch.int64, device="cuda")
+    return size_set, slots, slot_sz, acc
+
+
+@pytest.mark.parametrize("n,memory", [(65536, 256 << 20), (1 << 20, 1 << 30)])
+def test_phase_run_matches_replay(torch_cuda, n, memory):
+    torch = torch_cuda
+    nslots, seed, periods = 4, 0x5EED, 5
+    target = int(0.91 * nslots * n)
+    want = PhaseReplay(n, nslots, seed, SIZES).run(periods, THR95, THR95, target, 64)
+    with allocator(memory=memory) as H:
+        size_set, slots, slot_sz, acc = buffers(torch, n, nslots)
+        got = H.phase_run(n, nslots, seed, periods, THR95, THR95, target, size_set,
+                          len(SIZES), slots, slot_sz, acc)
+        assert got["failed"] == 0
+        for k in ("alloc_rounds", "free_rounds", "filled", "mallocs", "frees"):
+            assert got[k] == want[k], k
+        assert got["written_sum"] == want["wsum"] and got["read_sum"] == want["rsum"]
+        assert got["written_sum"] == got["read_sum"]
+        st = H.stats()
+        assert st["used_chunks"] == 0 and st["status"] == 0
+
+
+def test_phase_state_after_alloc_round(torch_cuda):
+    """After an allocation round and a free round, the live blocks are valid
+    and the slab state is exactly what they imply."""
+    torch = torch_cuda
+    n, nslots, seed = 1 << 18, 4, 77
+    with allocator(memory=512 << 20) as H:
+        size_set, slots, slot_sz, acc = buffers(torch, n, nslots)
+        H.phase_round(0, n, nslots, seed, 0, THR95, slots, slot_sz, acc, size_set, len(SIZES))
+        H.phase_round(1, n, nslots, seed, 1, THR95 // 2, slots, slot_sz, acc)
+        H.phase_round(0, n, nslots, seed, 2, THR95, slots, slot_sz, acc, size_set, len(SIZES))
+        torch.cuda.synchronize()
+        p = slots.cpu().numpy()
+        sz = slot_sz.cpu().numpy().astype(np.int64)
+        st = H.stats()
+        check_blocks(p, np.where(p != 0, sz, 0), st["pool_base"], st["pool_bytes"],
+                     allow_null=True)
+        dump = H.dump_state()
+        counts, bits, nib = expected_slab_state(p, np.where(p != 0, sz, 0), dump["pool_base"],
+                                                dump["sb_sz"], dump["nsbs"])
+        assert np.array_equal(dump["counters"] >> 12, counts)
+        assert np.array_equal(dump["bits"], bits)
+        assert np.array_equal(nibbles_to_chunk_layout(dump["nibbles"], dump["chunk_enc"]), nib)
+        a = acc.cpu().numpy()
+        assert a[1] == 0 and a[2] - a[3] > 0  # live blocks still hold their payload
+        H.phase_round(1, n, nslots, seed, 3, 0xFFFFFFFF, slots, slot_sz, acc)
+        torch.cuda.synchronize()
+        a = acc.cpu().numpy()
+        assert a[2] == a[3] and a[4] == a[5]
+        assert H.stats()["used_chunks"] == 0 and H.status() == 0
