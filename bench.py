@@ -260,9 +260,46 @@ def run_ours(args, rank, world, local_rank):
                               "failed_allocs": cnf,
                               "heap_bytes": H.stats()["cuda_heap_bytes"]}
     H.shutdown()
-    if rank == 0 and not args.only_gpu and not args.skip_phase:
-        res["phase"] = run_phase(torch, H, 3, hbm_peak())
+    if rank == 0 and not args.only_gpu:
+        if not args.skip_phase:
+            res["phase"] = run_leg("phase")
+        if not args.skip_batched:
+            res["batched"] = run_leg("batched")
+        if not args.skip_graph:
+            res["graph"] = run_leg("graph")
+        if not args.skip_serve:
+            res["serve"] = run_leg("serve")
     return res
+
+
+def run_leg(name: str) -> dict:
+    """A secondary workload in a child process: its own CUDA context, so
+    its pool and CUDA-heap sizes are set afresh."""
+    try:
+        p = subprocess.run([sys.executable, os.path.abspath(__file__), "--leg", name],
+                           capture_output=True, text=True, timeout=900)
+    except subprocess.TimeoutExpired:
+        return {"error": "timed out"}
+    for line in p.stdout.splitlines():
+        if line.startswith("LEG "):
+            return json.loads(line[4:])
+    return {"error": (p.stderr or p.stdout)[-600:]}
+
+
+def leg_main(args):
+    import torch
+
+    import halloc_b200 as H
+    torch.cuda.set_device(0)
+    if args.leg == "phase":
+        out = run_phase(torch, H, 3, hbm_peak())
+    elif args.leg == "graph":
+        out = run_graph(torch, H, 3)
+    elif args.leg == "serve":
+        out = run_serve(torch, H)
+    else:
+        out = run_batched(torch, H, 3, not args.no_tune)
+    print("LEG " + json.dumps(out), flush=True)
 
 
 PHASE_SIZES = [16, 24, 32, 48, 64, 96, 128, 192, 256]
@@ -310,6 +347,150 @@ def run_phase(torch, H, reps: int, hbm_peak_gbs: float | None) -> dict:
     if hbm_peak_gbs:
         out["payload"]["frac_of_hbm"] = gbs / hbm_peak_gbs
     return out
+
+
+BATCH_POOL, BATCH_HF = 4 << 30, 0.5
+
+
+def run_batched(torch, H, reps: int, tune: bool) -> dict:
+    """Batched request stream (64 batches, log-uniform 1,024..1,048,576
+    requests, geometric size classes p=0.3, 1 % large 4..64 KiB, lifetimes
+    1..8 batches) served by per-batch launches and by one graph-captured
+    persistent launch; then the autotuner sweep."""
+    from halloc_b200.autotune import autotune
+    from halloc_b200.workloads import BatchedRunner, batched_plan
+    plan = batched_plan(seed=1)
+    runner = BatchedRunner(plan, torch)
+    stream = torch.cuda.current_stream()
+    H.init(H.HallocOpts(memory=BATCH_POOL, halloc_fraction=BATCH_HF))
+    H.l2_persist(stream)
+
+    def timed(fn) -> list:
+        fn()
+        torch.cuda.synchronize()
+        runner.verify()
+        out = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            runner.verify()
+            out.append(e0.elapsed_time(e1))
+        return out
+
+    plain = timed(lambda: runner.plain(block=256, stream=stream))
+    try:
+        h = runner.prepare(block=256, task_items=2048, graph=True)
+        pers = timed(lambda: runner.launch(h, stream))
+    except Exception as e:  # report the plain form even so
+        runner.release()
+        H.shutdown()
+        return {"error": f"persistent form: {e}", "plain_ms": plain}
+    runner.release()
+    ok = H.status() == 0 and H.stats()["used_chunks"] == 0
+    H.shutdown()
+    n = plan.nreq
+    res = {"metric": "batched malloc/free pairs/s", "unit": "pairs/s", "requests": n,
+           "batches": plan.nbatch, "large_requests": int((plan.req_size > 3072).sum()),
+           "plain": {"value": n / (min(plain) * 1e-3), "ms": plain,
+                     "launches": int(np.count_nonzero(np.diff(plan.free_start))) +
+                     int(np.count_nonzero(np.diff(plan.batch_start)))},
+           "persistent_graph": {"value": n / (min(pers) * 1e-3), "ms": pers, "launches": 1,
+                                "block": 256, "task_items": 2048},
+           "speedup": min(plain) / min(pers), "ok": ok,
+           "pool": {"memory": BATCH_POOL, "halloc_fraction": BATCH_HF}}
+    if tune:
+        t = autotune(torch, runner, BATCH_POOL, BATCH_HF, reps=2)
+        t["best"]["value"] = n / (t["best"]["ms"] * 1e-3)
+        t["best"]["speedup_vs_plain"] = min(plain) / t["best"]["ms"]
+        res["autotune"] = t
+    return res
+
+
+SERVE_POOL = 16 << 30
+SERVE_POINTS = ((1e6, 1_000_000), (1e7, 2_000_000), (1e8, 10_000_000))
+
+
+def run_serve(torch, H) -> dict:
+    """Serving loop: Poisson arrivals at rate lambda of jobs that grow by 1..32
+    blocks of 256 B per step up to ceil(L/256), L log-uniform 64 B..2 MiB,
+    and live Exp(mean 50 steps); admission refused while the 12 GiB slab
+    pool of a 16 GiB pool is over 90 % full; one persistent kernel."""
+    H.init(H.HallocOpts(memory=SERVE_POOL))
+    out = {"metric": "serving jobs/s and hamalloc latency", "points": []}
+    ok = True
+    for lam, njobs in SERVE_POINTS:
+        res = torch.zeros(2 * njobs, dtype=torch.int64, device="cuda")
+        r = H.serve_run(res, njobs, lam, seed=7)
+        ok &= r["jobs_done"] == njobs and r["timeouts"] == 0
+        cpn = r["cycles_per_ns"] or 1.0
+        out["points"].append({
+            "lambda": lam, "jobs": njobs, "jobs_per_s": r["jobs_done"] / r["seconds"],
+            "seconds": r["seconds"], "allocs": r["allocs"],
+            "allocs_per_s": r["allocs"] / r["seconds"],
+            "alloc_failures": r["alloc_failures"], "refusals": r["refusals"],
+            "peak_occupancy": r["peak_live_blocks"] * 256 / H.stats()["pool_bytes"],
+            "p50_ns": r["p50_cycles"] / cpn, "p99_ns": r["p99_cycles"] / cpn,
+            "max_ns": r["max_cycles"] / cpn, "p50_cycles": r["p50_cycles"],
+            "p99_cycles": r["p99_cycles"], "sm_ghz": cpn})
+        del res
+    ok &= H.status() == 0 and H.stats()["used_chunks"] == 0
+    H.shutdown()
+    out["ok"] = ok
+    out["config"] = ("jobs of ceil(L/256) 256-B blocks, L log-uniform 64 B..2 MiB, growing "
+                     "1..32 blocks per step, lifetime Exp(mean 50 steps), Poisson arrivals, "
+                     "admission refused above 0.9 occupancy of the slab pool (16 GiB pool, "
+                     "12 GiB of slabs), one persistent kernel, host-fed through mapped memory")
+    return out
+
+
+GRAPH_N, GRAPH_POOL = 1 << 20, 1 << 30
+
+
+def run_graph(torch, H, reps: int) -> dict:
+    """Random-graph build: 1,048,576 vertices, Poisson(16) out-degree from a
+    seed, one thread per vertex growing an int32 neighbour array by doubling
+    (malloc new, copy, hafree old); then a CSR gather that frees every
+    array."""
+    from halloc_b200.workloads import poisson_thresholds
+    t = poisson_thresholds(16.0)
+    H.init(H.HallocOpts(memory=GRAPH_POOL))
+    stream = torch.cuda.current_stream()
+    n = GRAPH_N
+    cdf = torch.from_numpy(t.view(np.int32)).cuda()
+    arr = torch.zeros(n, dtype=torch.int64, device="cuda")
+    deg = torch.zeros(n, dtype=torch.int32, device="cuda")
+    acc = torch.zeros(3, dtype=torch.int64, device="cuda")
+    off = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    cols = torch.zeros(20 * n, dtype=torch.int32, device="cuda")
+    build_ms, gather_ms, edges, ok = [], [], 0, True
+    for r in range(reps + 1):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        H.graph_build(n, 0xC0FFEE + r, cdf, len(t), arr, deg, acc, stream)
+        e1.record(stream)
+        off[1:] = torch.cumsum(deg.to(torch.int64), 0)
+        e1b = torch.cuda.Event(enable_timing=True)
+        e1b.record(stream)
+        H.graph_gather(n, arr, deg, off, cols, stream)
+        e2.record(stream)
+        e2.synchronize()
+        failed, grows, ne = acc.cpu().tolist()
+        ok &= failed == 0 and ne == int(off[-1])
+        if r:
+            build_ms.append(e0.elapsed_time(e1))
+            gather_ms.append(e1b.elapsed_time(e2))
+            edges += ne
+    ok &= H.status() == 0 and H.stats()["used_chunks"] == 0
+    H.shutdown()
+    return {"metric": "graph-build edges/s", "unit": "edges/s",
+            "value": edges / (sum(build_ms) * 1e-3), "build_ms": build_ms,
+            "gather_free_ms": gather_ms, "edges_per_run": edges // reps, "ok": ok,
+            "config": "n=1,048,576, Poisson(16) out-degree from a seed on the device, "
+                      "int32 arrays from capacity 2 doubling (malloc new, copy, hafree old); "
+                      "gather = CSR copy + hafree of every array"}
 
 
 def hbm_peak() -> float | None:
@@ -397,6 +578,9 @@ def main_ours(args):
             "vs_cuda_malloc": value / world / res["cuda_malloc"]["value"]
             if res.get("cuda_malloc") else None,
             "phase": res.get("phase"),
+            "batched": res.get("batched"),
+            "graph": res.get("graph"),
+            "serve": res.get("serve"),
             "gpu_launches": args.steps,
             "clocks": res["clocks"],
         }
@@ -448,12 +632,20 @@ def main():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--skip-phase", action="store_true", help="skip the mixed-size phase leg")
+    p.add_argument("--skip-batched", action="store_true", help="skip the batched leg")
+    p.add_argument("--no-tune", action="store_true", help="batched leg without the autotuner")
+    p.add_argument("--skip-graph", action="store_true", help="skip the random-graph leg")
+    p.add_argument("--skip-serve", action="store_true", help="skip the serving leg")
+    p.add_argument("--leg", choices=["phase", "batched", "graph", "serve"],
+                   help=argparse.SUPPRESS)
     p.add_argument("--only-gpu", action="store_true",
                    help="skip the CPU and CUDA-malloc legs (profiling runs)")
     args = p.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.leg:
+        leg_main(args)
+    elif args.impl == "reference":
         main_reference(args)
     else:
         main_ours(args)

@@ -23,8 +23,9 @@ import numpy as np
 __all__ = [
     "HallocError", "HallocOpts", "init", "shutdown", "extfrag", "stats", "status",
     "clear_status", "set_wait_limit", "dump_state", "l2_persist", "malloc_batch",
-    "free_batch", "phase_round", "phase_run", "throughput", "throughput_host", "cuda_throughput", "trace",
-    "atomic_peak", "debug_set_head_lock", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
+    "free_batch", "phase_round", "phase_run", "graph_build", "graph_gather", "serve_run",
+    "throughput", "throughput_host", "cuda_throughput", "trace",
+    "atomic_peak", "debug_set_head_lock", "set_hash_scale", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
 ]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -81,6 +82,29 @@ class _CPhaseResult(ctypes.Structure):
                 ("acc", ctypes.c_uint64 * 6)]
 
 
+SERVE_HIST = 1024
+
+
+class _CServeCfg(ctypes.Structure):
+    _fields_ = [("njobs", ctypes.c_uint32), ("seed", ctypes.c_uint32),
+                ("lam", ctypes.c_double), ("occupancy_limit", ctypes.c_double),
+                ("mean_life", ctypes.c_double), ("block_bytes", ctypes.c_uint32),
+                ("min_len", ctypes.c_uint32), ("max_len", ctypes.c_uint32),
+                ("grow_min", ctypes.c_uint32), ("grow_max", ctypes.c_uint32),
+                ("cta_threads", ctypes.c_uint32), ("ctas_per_sm", ctypes.c_uint32),
+                ("job_ids", ctypes.c_void_p), ("njob_ids", ctypes.c_uint32),
+                ("results", ctypes.c_void_p)]
+
+
+class _CServeResult(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("cycles_per_ns", ctypes.c_double),
+                ("jobs_done", ctypes.c_uint64), ("allocs", ctypes.c_uint64),
+                ("alloc_failures", ctypes.c_uint64), ("refusals", ctypes.c_uint64),
+                ("peak_live_blocks", ctypes.c_uint64), ("timeouts", ctypes.c_uint64),
+                ("p50_cycles", ctypes.c_double), ("p99_cycles", ctypes.c_double),
+                ("max_cycles", ctypes.c_double), ("hist", ctypes.c_uint64 * SERVE_HIST)]
+
+
 class _CDump(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in (
         "tickets", "heads", "cached", "size_infos", "counters", "size_id", "chunk_id",
@@ -99,6 +123,10 @@ _SIGS = {
     "ha_dump_state_c": (_int, [ctypes.POINTER(_CDump)]),
     "ha_l2_persist_c": (_int, [_vp]),
     "ha_debug_set_head_lock_c": (_int, [_u32, _u32]),
+    "ha_set_hash_scale_c": (_int, [_u32]),
+    "ha_serve_run_c": (_int, [ctypes.POINTER(_CServeCfg), ctypes.POINTER(_CServeResult), _vp]),
+    "ha_graph_build_c": (_int, [_u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
+    "ha_graph_gather_c": (_int, [_u32, _vp, _vp, _vp, _vp, _vp]),
     "ha_malloc_batch_c": (_int, [_vp, _u32, _u32, _vp, _int, _vp]),
     "ha_free_batch_c": (_int, [_vp, _u32, _u32, _vp]),
     "ha_throughput_c": (_int, [_vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp]),
@@ -229,6 +257,11 @@ def dump_state() -> dict:
     return arrs
 
 
+def set_hash_scale(percent: int) -> None:
+    """Hash-step scale for the next init (100 = the reference's rule)."""
+    _check(load().ha_set_hash_scale_c(percent), "ha_set_hash_scale_c")
+
+
 def debug_set_head_lock(size_id: int, held: bool) -> None:
     """Failure-detection test hook (see ha_debug_set_head_lock_c)."""
     _check(load().ha_debug_set_head_lock_c(size_id, 1 if held else 0),
@@ -298,6 +331,41 @@ def phase_run(nthreads: int, nslots: int, seed: int, periods: int, thr_alloc: in
     out = {"alloc_rounds": r.alloc_rounds, "free_rounds": r.free_rounds,
            "kernel_ms": r.kernel_ms, "filled": r.filled}
     out.update(dict(zip(PHASE_ACC, list(r.acc))))
+    return out
+
+
+def graph_build(n: int, seed: int, cdf, ncdf: int, arr, deg, acc, stream=None) -> None:
+    """Random-graph build with doubling neighbour arrays (ha_graph_build_c)."""
+    _check(load().ha_graph_build_c(n, seed, _addr(cdf), ncdf, _addr(arr), _addr(deg),
+                                   _addr(acc), _stream(stream)), "ha_graph_build_c")
+
+
+def graph_gather(n: int, arr, deg, offsets, cols, stream=None) -> None:
+    """CSR gather of the graph, freeing every neighbour array."""
+    _check(load().ha_graph_gather_c(n, _addr(arr), _addr(deg), _addr(offsets), _addr(cols),
+                                    _stream(stream)), "ha_graph_gather_c")
+
+
+def serve_run(results, njobs: int, lam: float, seed: int = 1, occupancy_limit: float = 0.9,
+              mean_life: float = 50.0, block_bytes: int = 256, min_len: int = 64,
+              max_len: int = 2 << 20, grow_min: int = 1, grow_max: int = 32,
+              cta_threads: int = 256, ctas_per_sm: int = 0, job_ids=None,
+              stream=None) -> dict:
+    """Serving loop (ha_serve_run_c).  results: device buffer of 2*njobs
+    uint64 (blocks, value sum per job id).  job_ids: optional host sequence
+    of ids to release instead of 0..njobs-1."""
+    ids = None
+    if job_ids is not None:
+        ids = np.ascontiguousarray(np.asarray(job_ids, dtype=np.uint32))
+    cfg = _CServeCfg(njobs, seed, lam, occupancy_limit, mean_life, block_bytes, min_len,
+                     max_len, grow_min, grow_max, cta_threads, ctas_per_sm,
+                     ids.ctypes.data if ids is not None else None,
+                     len(ids) if ids is not None else 0, _addr(results))
+    r = _CServeResult()
+    _check(load().ha_serve_run_c(ctypes.byref(cfg), ctypes.byref(r), _stream(stream)),
+           "ha_serve_run_c")
+    out = {f: getattr(r, f) for f, _ in _CServeResult._fields_ if f != "hist"}
+    out["hist"] = np.frombuffer(bytes(r.hist), dtype=np.uint64).copy()
     return out
 
 

@@ -35,7 +35,8 @@ HEADERS = [os.path.join(CSRC, f) for f in ("ha_core.cuh", "ha_types.h")] + [
 # that calls hamalloc/hafree inherits the callee's register count at device
 # link time, so this bounds the occupancy cost for user kernels (the
 # reference built with the same cap).
-SOURCES = {"halloc.cu": ["-maxrregcount=64"], "ha_kernels.cu": []}
+SOURCES = {"halloc.cu": ["-maxrregcount=64"], "ha_kernels.cu": [],
+           "ha_serve.cu": ["-maxrregcount=64"]}
 
 
 def nvcc() -> str:

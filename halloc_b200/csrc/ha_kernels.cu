@@ -9,6 +9,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <vector>
+
 #include "halloc.h"
 #include "halloc_c.h"
 
@@ -233,6 +235,194 @@ __global__ void ha_phase_free_k(uint32_t n, uint32_t nslots, uint32_t seed, uint
   block_add2(nfree, 0, acc + 5, acc + 5);
 }
 
+// ---- batched workload ---------------------------------------------------------
+
+// allocation of requests [begin, end): the block carries its request id
+__device__ __forceinline__ void batched_malloc_one(uint32_t r, const uint32_t *req_size,
+                                                   unsigned long long *req_ptr,
+                                                   unsigned long long &nfail,
+                                                   unsigned long long &nmal) {
+  void *p = hamalloc(req_size[r]);
+  req_ptr[r] = (unsigned long long)(uintptr_t)p;
+  if (p) {
+    *reinterpret_cast<unsigned long long *>(p) = r;
+    nmal++;
+  } else {
+    nfail++;
+  }
+}
+
+__device__ __forceinline__ void batched_free_one(uint32_t k, const uint32_t *free_ids,
+                                                 unsigned long long *req_ptr,
+                                                 unsigned long long &bad,
+                                                 unsigned long long &idsum,
+                                                 unsigned long long &nfree) {
+  const uint32_t r = free_ids[k];
+  void *p = (void *)(uintptr_t)req_ptr[r];
+  if (!p) return;
+  if (*reinterpret_cast<const unsigned long long *>(p) != r) bad++;
+  idsum += r;
+  nfree++;
+  hafree(p);
+  req_ptr[r] = 0;  // a later run (graph replay) starts from all-NULL pointers
+}
+
+__global__ void ha_bmalloc_k(uint32_t begin, uint32_t end, const uint32_t *req_size,
+                             unsigned long long *req_ptr, unsigned long long *acc) {
+  const uint32_t r = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long nfail = 0, nmal = 0;
+  if (r < end) batched_malloc_one(r, req_size, req_ptr, nfail, nmal);
+  block_add2(nfail, nmal, acc, acc + 3);
+}
+
+__global__ void ha_bfree_k(uint32_t begin, uint32_t end, const uint32_t *free_ids,
+                           unsigned long long *req_ptr, unsigned long long *acc) {
+  const uint32_t k = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long bad = 0, idsum = 0, nfree = 0;
+  if (k < end) batched_free_one(k, free_ids, req_ptr, bad, idsum, nfree);
+  block_add2(bad, idsum, acc + 1, acc + 2);
+  block_add2(nfree, 0, acc + 4, acc + 4);
+}
+
+struct BatchTask {
+  uint32_t begin, end;  // range of request ids (malloc) or free_ids slots (free)
+  uint32_t step;        // the step (= batch of an allocation task)
+  uint32_t is_free;
+};
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const unsigned int *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Persistent form.  ctl[0] = next task; ctl[1 + b] = finished allocation
+// tasks of batch b; btasks[b] = allocation tasks of batch b.  A free task of
+// step s starts once every batch b < s is complete; each block remembers the
+// batches it has already seen complete (tasks reach a block in step order).
+__global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uint32_t *btasks,
+                              const uint32_t *req_size, unsigned long long *req_ptr,
+                              const uint32_t *free_ids, unsigned int *ctl,
+                              unsigned long long *acc) {
+  __shared__ uint32_t s_task, s_done_below;
+  unsigned long long nfail = 0, nmal = 0, bad = 0, idsum = 0, nfree = 0, late = 0;
+  if (threadIdx.x == 0) s_done_below = 0;
+  for (;;) {
+    __syncthreads();  // everyone has read s_task
+    if (threadIdx.x == 0) s_task = atomicAdd(&ctl[0], 1u);
+    __syncthreads();
+    const uint32_t t = s_task;
+    if (t >= ntasks) break;
+    const BatchTask tk = tasks[t];
+    if (tk.is_free) {
+      if (threadIdx.x == 0) {
+        // every allocation task of those batches was dequeued earlier by a
+        // running block, so each wait ends
+        const uint64_t limit = now_ns() + 2000000000ull;
+        uint32_t b = s_done_below;
+        while (b < tk.step) {
+          if (ld_acquire_u32(&ctl[1 + b]) >= btasks[b]) {
+            b++;
+            continue;
+          }
+          if (now_ns() > limit) {
+            late++;
+            break;
+          }
+          __nanosleep(128);
+        }
+        s_done_below = b;
+      }
+      __syncthreads();
+      for (uint32_t k = tk.begin + threadIdx.x; k < tk.end; k += blockDim.x)
+        batched_free_one(k, free_ids, req_ptr, bad, idsum, nfree);
+    } else {
+      for (uint32_t r = tk.begin + threadIdx.x; r < tk.end; r += blockDim.x)
+        batched_malloc_one(r, req_size, req_ptr, nfail, nmal);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();  // this block's req_ptr and payload writes before the count
+        atomicAdd(&ctl[1 + tk.step], 1u);
+      }
+    }
+  }
+  block_add2(nfail, nmal, acc, acc + 3);
+  block_add2(bad, idsum, acc + 1, acc + 2);
+  block_add2(nfree, late, acc + 4, acc + 5);
+}
+
+// ---- random-graph build -----------------------------------------------------
+//
+// Vertex u draws its out-degree d from a Poisson CDF given as 32-bit
+// thresholds (d = number of thresholds <= mix32(u ^ seed)), and its k-th
+// neighbour as mix32(mix32(u ^ seed ^ 0xABCDEF01) + k * 0x9E3779B9) mod n.
+// One thread per vertex appends its neighbours to an int32 array from
+// hamalloc, starting at capacity 2 and doubling (malloc new, copy, free old).
+
+__device__ __forceinline__ uint32_t graph_degree(uint32_t u, uint32_t seed, const uint32_t *cdf,
+                                                 uint32_t ncdf) {
+  const uint32_t h = mix32(u ^ seed);
+  uint32_t d = 0;
+  while (d < ncdf && cdf[d] <= h) d++;
+  return d;
+}
+__device__ __forceinline__ uint32_t graph_neighbour(uint32_t u, uint32_t k, uint32_t seed,
+                                                    uint32_t n) {
+  return mix32(mix32(u ^ seed ^ 0xABCDEF01u) + k * 0x9E3779B9u) % n;
+}
+
+// acc: [0] failed allocations, [1] reallocations (doublings), [2] edges
+__global__ void ha_graph_build_k(uint32_t n, uint32_t seed, const uint32_t *cdf, uint32_t ncdf,
+                                 unsigned long long *arr, uint32_t *deg,
+                                 unsigned long long *acc) {
+  const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long nfail = 0, ngrow = 0, nedge = 0;
+  if (u < n) {
+    const uint32_t d = graph_degree(u, seed, cdf, ncdf);
+    uint32_t cap = 2, cnt = 0;
+    uint32_t *a = (uint32_t *)hamalloc(cap * sizeof(uint32_t));
+    if (!a) nfail++;
+    for (uint32_t k = 0; k < d && a; k++) {
+      if (cnt == cap) {
+        uint32_t *b = (uint32_t *)hamalloc(2 * cap * sizeof(uint32_t));
+        if (!b) {
+          nfail++;
+          break;
+        }
+        for (uint32_t j = 0; j < cnt; j++) b[j] = a[j];
+        hafree(a);
+        a = b;
+        cap *= 2;
+        ngrow++;
+      }
+      a[cnt++] = graph_neighbour(u, k, seed, n);
+    }
+    arr[u] = (unsigned long long)(uintptr_t)a;
+    deg[u] = cnt;
+    nedge = cnt;
+  }
+  block_add2(nfail, ngrow, acc, acc + 1);
+  block_add2(nedge, 0, acc + 2, acc + 2);
+}
+
+// Copies each vertex's array into CSR columns at offsets[u] and frees it.
+__global__ void ha_graph_gather_k(uint32_t n, unsigned long long *arr, const uint32_t *deg,
+                                  const unsigned long long *offsets, uint32_t *cols) {
+  const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  uint32_t *a = (uint32_t *)(uintptr_t)arr[u];
+  if (!a) return;
+  const unsigned long long o = offsets[u];
+  for (uint32_t k = 0; k < deg[u]; k++) cols[o + k] = a[k];
+  hafree(a);
+  arr[u] = 0;
+}
+
 // serial replay on one thread
 __global__ void ha_trace_k(const int64_t *ops, int64_t n, int64_t *out) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
@@ -406,6 +596,177 @@ extern "C" int ha_phase_run_c(uint32_t nthreads, uint32_t nslots, uint32_t seed,
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
+}
+
+extern "C" int ha_batched_plain_c(const ha_batch_plan_t *plan, uint32_t block, void *stream) {
+  if (!plan || !plan->acc || !plan->h_batch_start || !plan->h_free_start || block == 0 ||
+      block > 1024)
+    return HA_EINVAL;
+  cudaStream_t s = as_stream(stream);
+  unsigned long long *acc = reinterpret_cast<unsigned long long *>(plan->acc);
+  if (cudaMemsetAsync(acc, 0, 8 * sizeof(uint64_t), s) != cudaSuccess) return HA_ECUDA;
+  unsigned long long *rp = reinterpret_cast<unsigned long long *>(plan->req_ptr);
+  for (uint32_t st = 0; st <= plan->nbatch; st++) {
+    const uint32_t f0 = plan->h_free_start[st], f1 = plan->h_free_start[st + 1];
+    if (f1 > f0)
+      ha_bfree_k<<<blocks_for(f1 - f0, block), block, 0, s>>>(f0, f1, plan->free_ids, rp, acc);
+    if (st < plan->nbatch) {
+      const uint32_t b0 = plan->h_batch_start[st], b1 = plan->h_batch_start[st + 1];
+      if (b1 > b0)
+        ha_bmalloc_k<<<blocks_for(b1 - b0, block), block, 0, s>>>(b0, b1, plan->req_size, rp,
+                                                                 acc);
+    }
+  }
+  return launch_status();
+}
+
+namespace {
+struct Batched {
+  ha_batch_plan_t plan;
+  BatchTask *tasks;
+  uint32_t ntasks;
+  uint32_t *btasks;  // allocation tasks per batch
+  unsigned int *ctl; // next task, then finished allocation tasks per batch
+  uint32_t grid, block;
+  cudaGraphExec_t exec;
+  bool graph;
+};
+
+void enqueue_persistent(const Batched *b, cudaStream_t s) {
+  unsigned long long *acc = reinterpret_cast<unsigned long long *>(b->plan.acc);
+  cudaMemsetAsync(acc, 0, 8 * sizeof(uint64_t), s);
+  cudaMemsetAsync(b->ctl, 0, (b->plan.nbatch + 1) * sizeof(unsigned int), s);
+  ha_bpersist_k<<<b->grid, b->block, 0, s>>>(
+      b->tasks, b->ntasks, b->btasks, b->plan.req_size,
+      reinterpret_cast<unsigned long long *>(b->plan.req_ptr), b->plan.free_ids, b->ctl, acc);
+}
+
+void release_batched(Batched *b) {
+  if (!b) return;
+  if (b->graph) cudaGraphExecDestroy(b->exec);
+  cudaFree(b->tasks);
+  cudaFree(b->btasks);
+  cudaFree(b->ctl);
+  delete b;
+}
+}  // namespace
+
+extern "C" int ha_batched_prepare_c(const ha_batch_plan_t *plan, uint32_t block,
+                                    uint32_t ctas_per_sm, uint32_t task_items, int use_graph,
+                                    void **out) {
+  if (!plan || !out || !plan->acc || !plan->h_batch_start || !plan->h_free_start ||
+      block == 0 || block > 1024 || block % 32 || task_items == 0)
+    return HA_EINVAL;
+  *out = nullptr;
+  // task table: for each step its free chunks, then its allocation chunks
+  std::vector<BatchTask> tasks;
+  std::vector<uint32_t> btasks(plan->nbatch + 1, 0);
+  for (uint32_t st = 0; st <= plan->nbatch; st++) {
+    for (uint32_t k = plan->h_free_start[st]; k < plan->h_free_start[st + 1]; k += task_items) {
+      uint32_t e = k + task_items < plan->h_free_start[st + 1] ? k + task_items
+                                                                : plan->h_free_start[st + 1];
+      tasks.push_back({k, e, st, 1u});
+    }
+    if (st == plan->nbatch) break;
+    for (uint32_t r = plan->h_batch_start[st]; r < plan->h_batch_start[st + 1];
+         r += task_items) {
+      uint32_t e = r + task_items < plan->h_batch_start[st + 1] ? r + task_items
+                                                                : plan->h_batch_start[st + 1];
+      tasks.push_back({r, e, st, 0u});
+      btasks[st]++;
+    }
+  }
+  int dev = 0, nsm = 0, fit = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, ha_bpersist_k, (int)block, 0) !=
+          cudaSuccess || fit <= 0)
+    return HA_ECUDA;
+  Batched *b = new Batched();
+  b->plan = *plan;
+  b->plan.h_batch_start = nullptr;  // not kept
+  b->plan.h_free_start = nullptr;
+  b->ntasks = (uint32_t)tasks.size();
+  b->block = block;
+  b->grid = (uint32_t)nsm * (ctas_per_sm && ctas_per_sm < (uint32_t)fit ? ctas_per_sm : fit);
+  if (cudaMalloc(&b->tasks, sizeof(BatchTask) * (tasks.empty() ? 1 : tasks.size())) !=
+          cudaSuccess ||
+      cudaMalloc(&b->btasks, sizeof(uint32_t) * btasks.size()) != cudaSuccess ||
+      cudaMalloc(&b->ctl, (plan->nbatch + 1) * sizeof(unsigned int)) != cudaSuccess ||
+      cudaMemcpy(b->tasks, tasks.data(), sizeof(BatchTask) * tasks.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->btasks, btasks.data(), sizeof(uint32_t) * btasks.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    release_batched(b);
+    return HA_ECUDA;
+  }
+  if (use_graph) {
+    cudaStream_t cap;
+    cudaGraph_t g;
+    if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
+      release_batched(b);
+      return HA_ECUDA;
+    }
+    bool ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      enqueue_persistent(b, cap);
+      ok = cudaStreamEndCapture(cap, &g) == cudaSuccess;
+    }
+    if (ok) {
+      ok = cudaGraphInstantiate(&b->exec, g, 0) == cudaSuccess;
+      cudaGraphDestroy(g);
+    }
+    cudaStreamDestroy(cap);
+    if (!ok) {
+      cudaGetLastError();
+      release_batched(b);
+      return HA_ECUDA;
+    }
+    b->graph = true;
+  }
+  *out = b;
+  return HA_OK;
+}
+
+extern "C" int ha_batched_launch_c(void *handle, void *stream) {
+  if (!handle) return HA_EINVAL;
+  Batched *b = static_cast<Batched *>(handle);
+  cudaStream_t s = as_stream(stream);
+  if (b->graph) {
+    if (cudaGraphLaunch(b->exec, s) != cudaSuccess) return launch_status();
+    return HA_OK;
+  }
+  enqueue_persistent(b, s);
+  return launch_status();
+}
+
+extern "C" int ha_batched_release_c(void *handle) {
+  if (!handle) return HA_EINVAL;
+  release_batched(static_cast<Batched *>(handle));
+  return HA_OK;
+}
+
+extern "C" int ha_graph_build_c(uint32_t n, uint32_t seed, const uint32_t *cdf, uint32_t ncdf,
+                                uint64_t *arr, uint32_t *deg, uint64_t *acc, void *stream) {
+  if (!cdf || !ncdf || !arr || !deg || !acc) return HA_EINVAL;
+  if (n == 0) return HA_OK;
+  cudaStream_t s = as_stream(stream);
+  if (cudaMemsetAsync(acc, 0, 3 * sizeof(uint64_t), s) != cudaSuccess) return HA_ECUDA;
+  ha_graph_build_k<<<blocks_for(n, 128), 128, 0, s>>>(
+      n, seed, cdf, ncdf, reinterpret_cast<unsigned long long *>(arr), deg,
+      reinterpret_cast<unsigned long long *>(acc));
+  return launch_status();
+}
+
+extern "C" int ha_graph_gather_c(uint32_t n, uint64_t *arr, const uint32_t *deg,
+                                 const uint64_t *offsets, uint32_t *cols, void *stream) {
+  if (!arr || !deg || !offsets || !cols) return HA_EINVAL;
+  if (n == 0) return HA_OK;
+  ha_graph_gather_k<<<blocks_for(n, 128), 128, 0, as_stream(stream)>>>(
+      n, reinterpret_cast<unsigned long long *>(arr), deg,
+      reinterpret_cast<const unsigned long long *>(offsets), cols);
+  return launch_status();
 }
 
 extern "C" int ha_trace_c(const int64_t *ops, int64_t n, int64_t *out, void *stream) {

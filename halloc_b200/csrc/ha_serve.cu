@@ -1,0 +1,388 @@
+// ha_serve.cu -- serving loop: a host-fed job stream served by continuous
+// batching in one persistent kernel (ha_serve_run_c, halloc_c.h).
+//
+// Jobs are ids; every parameter derives from a hash of (seed, id), so a
+// job's result does not depend on what else runs beside it.  A host thread
+// releases ids at Poisson arrival times through a counter in mapped host
+// memory.  Each thread of the persistent kernel owns one job slot; a block
+// claims released jobs for its empty slots while the slab pool is at most
+// `occupancy_limit` full, then advances every active job by one step:
+// grow by 1..32 blocks of 256 B (hamalloc, linked through the blocks), and
+// at the end of the job's lifetime read its blocks back and hafree them.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <chrono>
+#include <random>
+#include <vector>
+
+#include "halloc.h"
+#include "halloc_c.h"
+
+namespace {
+
+struct ServeCtl {  // mapped host memory, written by the host
+  uint32_t released;  // ids order[0 .. released) may be claimed
+  uint32_t ended;     // nothing more will be released
+};
+
+struct ServeDev {  // device memory
+  uint32_t claimed;  // next index of order[] to hand out
+  uint32_t pad;
+  unsigned long long live_blocks, peak_live;
+  unsigned long long jobs_done, allocs, failures, refusals, timeouts;
+  unsigned long long cycles, nanos;
+  unsigned long long hist[HA_SERVE_HIST];
+};
+
+struct ServeParams {
+  const uint32_t *order;
+  uint32_t norder;
+  uint32_t seed;
+  uint32_t block_bytes;
+  float log_min, log_span;  // log-uniform job length
+  float mean_life;
+  uint32_t grow_min, grow_span;
+  unsigned long long live_limit;  // admission: live blocks must be <= this
+  unsigned long long *results;
+  const ServeCtl *ctl;  // device view of the mapped host struct
+  ServeDev *dev;
+};
+
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+__device__ __forceinline__ uint32_t ld_acquire_sys(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// log-linear latency bucket: 16 buckets per power of two
+__device__ __forceinline__ uint32_t lat_bucket(unsigned long long c) {
+  if (c < 16) return (uint32_t)c;
+  const uint32_t e = 63 - __clzll(c);
+  const uint32_t b = (e - 3) * 16 + (uint32_t)((c >> (e - 4)) & 15);
+  return b < HA_SERVE_HIST ? b : HA_SERVE_HIST - 1;
+}
+
+struct Job {
+  uint32_t id, target, blocks, steps, life, h;
+};
+
+__device__ __forceinline__ void job_start(Job &j, uint32_t id, const ServeParams &P) {
+  j.id = id;
+  j.h = mix32(P.seed ^ mix32(id));
+  const float u1 = ((float)j.h + 0.5f) * 2.3283064e-10f;
+  const float len = expf(P.log_min + u1 * P.log_span);
+  j.target = max(1u, (uint32_t)ceilf(len / (float)P.block_bytes));
+  const float u2 = ((float)mix32(j.h ^ 0x51ED270Bu) + 0.5f) * 2.3283064e-10f;
+  j.life = max(1u, (uint32_t)ceilf(-P.mean_life * logf(u2)));
+  j.blocks = 0;
+  j.steps = 0;
+}
+
+__global__ void __launch_bounds__(1024) ha_serve_k(ServeParams P) {
+  __shared__ unsigned long long s_hist[HA_SERVE_HIST];
+  __shared__ uint32_t s_base, s_n, s_exit;
+  __shared__ uint32_t s_warp_empty[32];
+  for (uint32_t i = threadIdx.x; i < HA_SERVE_HIST; i += blockDim.x) s_hist[i] = 0;
+  const uint64_t ns0 = now_ns();
+  const long long cyc0 = clock64();
+  Job j;
+  j.id = 0xffffffffu;
+  void *head = nullptr;
+  unsigned long long vsum = 0, my_allocs = 0, my_fail = 0, my_done = 0;
+  uint64_t idle_since = 0;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    // ---- admission ------------------------------------------------------
+    const bool empty = j.id == 0xffffffffu;
+    const uint32_t em = __ballot_sync(0xffffffffu, empty);
+    if (lane == 0) s_warp_empty[warp] = __popc(em);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t nempty = 0;
+      for (uint32_t w = 0; w < (blockDim.x + 31) / 32; w++) nempty += s_warp_empty[w];
+      uint32_t base = 0, k = 0;
+      if (nempty) {
+        if (atomicAdd(&P.dev->live_blocks, 0ull) > P.live_limit) {
+          atomicAdd(&P.dev->refusals, 1ull);
+        } else {
+          for (;;) {
+            const uint32_t c = atomicAdd(&P.dev->claimed, 0u);
+            const uint32_t r = min(ld_acquire_sys(&P.ctl->released), P.norder);
+            k = r > c ? min(nempty, r - c) : 0;
+            if (!k || atomicCAS(&P.dev->claimed, c, c + k) == c) {
+              base = c;
+              break;
+            }
+          }
+        }
+      }
+      s_base = base;
+      s_n = k;
+    }
+    __syncthreads();
+    if (empty) {
+      // rank of this empty slot among the block's empty slots
+      uint32_t rank = __popc(em & ((1u << lane) - 1));
+      for (uint32_t w = 0; w < warp; w++) rank += s_warp_empty[w];
+      if (rank < s_n) {
+        job_start(j, P.order[s_base + rank], P);
+        head = nullptr;
+        vsum = 0;
+      }
+    }
+    // ---- one step of every active job -------------------------------------
+    uint32_t grown = 0, freed = 0;
+    if (j.id != 0xffffffffu) {
+      const uint32_t g =
+          P.grow_min + mix32(j.h + j.steps * 0x9E3779B9u) % P.grow_span;
+      for (uint32_t i = 0; i < g && j.blocks < j.target; i++) {
+        const long long t0 = clock64();
+        void *p = hamalloc(P.block_bytes);
+        const long long t1 = clock64();
+        atomicAdd(&s_hist[lat_bucket((unsigned long long)(t1 - t0))], 1ull);
+        my_allocs++;
+        if (!p) {
+          my_fail++;
+          break;
+        }
+        const uint32_t v = mix32(j.id * 0x27D4EB2Fu + j.blocks);
+        *reinterpret_cast<void **>(p) = head;
+        reinterpret_cast<uint32_t *>(p)[2] = v;
+        head = p;
+        j.blocks++;
+        grown++;
+      }
+      if (++j.steps >= j.life) {
+        for (void *p = head; p;) {
+          void *nx = *reinterpret_cast<void **>(p);
+          vsum += reinterpret_cast<const uint32_t *>(p)[2];
+          hafree(p);
+          p = nx;
+        }
+        P.results[2 * (size_t)j.id] = j.blocks;
+        P.results[2 * (size_t)j.id + 1] = vsum;
+        freed = j.blocks;
+        my_done++;
+        j.id = 0xffffffffu;
+        head = nullptr;
+      }
+    }
+    // live-block count, one atomic per warp
+    long long delta = (long long)grown - (long long)freed;
+    for (int o = 16; o > 0; o >>= 1) delta += __shfl_down_sync(0xffffffffu, delta, o);
+    if (lane == 0 && delta) {
+      const unsigned long long now =
+          atomicAdd(&P.dev->live_blocks, (unsigned long long)delta) + (unsigned long long)delta;
+      if (delta > 0) atomicMax(&P.dev->peak_live, now);
+    }
+    // ---- leave when the stream has ended and the block is idle -------------
+    const uint32_t active = __syncthreads_count(j.id != 0xffffffffu);
+    if (threadIdx.x == 0) {
+      uint32_t leave = 0;
+      if (active == 0 && s_n == 0) {
+        const bool ended = ld_acquire_sys(&P.ctl->ended) != 0;
+        if (ended && atomicAdd(&P.dev->claimed, 0u) >= P.norder) {
+          leave = 1;
+        } else {
+          const uint64_t t = now_ns();
+          if (!idle_since) idle_since = t;
+          if (t - idle_since > 5000000000ull) {  // nothing to do for 5 s
+            atomicAdd(&P.dev->timeouts, 1ull);
+            leave = 1;
+          } else {
+            __nanosleep(1000);
+          }
+        }
+      } else {
+        idle_since = 0;
+      }
+      s_exit = leave;
+    }
+    __syncthreads();
+    if (s_exit) break;
+  }
+  // ---- totals ---------------------------------------------------------------
+  for (int o = 16; o > 0; o >>= 1) {
+    my_allocs += __shfl_down_sync(0xffffffffu, my_allocs, o);
+    my_fail += __shfl_down_sync(0xffffffffu, my_fail, o);
+    my_done += __shfl_down_sync(0xffffffffu, my_done, o);
+  }
+  if (lane == 0) {
+    if (my_allocs) atomicAdd(&P.dev->allocs, my_allocs);
+    if (my_fail) atomicAdd(&P.dev->failures, my_fail);
+    if (my_done) atomicAdd(&P.dev->jobs_done, my_done);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < HA_SERVE_HIST; i += blockDim.x)
+    if (s_hist[i]) atomicAdd(&P.dev->hist[i], s_hist[i]);
+  if (threadIdx.x == 0) {
+    atomicAdd(&P.dev->cycles, (unsigned long long)(clock64() - cyc0));
+    atomicAdd(&P.dev->nanos, (unsigned long long)(now_ns() - ns0));
+  }
+}
+
+// lower bound of a histogram bucket, in cycles
+double bucket_value(uint32_t b) {
+  if (b < 16) return b;
+  const uint32_t e = b / 16 + 3, m = b % 16;
+  return (double)((16ull + m) << (e - 4));
+}
+
+double percentile(const unsigned long long *h, double q) {
+  unsigned long long total = 0;
+  for (int i = 0; i < HA_SERVE_HIST; i++) total += h[i];
+  if (!total) return 0;
+  const double want = q * (double)total;
+  unsigned long long run = 0;
+  for (int i = 0; i < HA_SERVE_HIST; i++) {
+    run += h[i];
+    if ((double)run >= want) {
+      // midpoint of the bucket
+      return 0.5 * (bucket_value(i) + bucket_value(i + 1));
+    }
+  }
+  return bucket_value(HA_SERVE_HIST - 1);
+}
+
+}  // namespace
+
+extern "C" int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out, void *stream) {
+  if (!cfg || !out || !cfg->results || cfg->block_bytes < 16 || cfg->block_bytes > 3072 ||
+      cfg->min_len == 0 || cfg->max_len < cfg->min_len || cfg->grow_min == 0 ||
+      cfg->grow_max < cfg->grow_min || !(cfg->lambda > 0) || !(cfg->mean_life > 0) ||
+      cfg->cta_threads == 0 || cfg->cta_threads > 1024 || cfg->cta_threads % 32)
+    return HA_EINVAL;
+  ha_stats_t st;
+  int rc = ha_stats_c(&st);
+  if (rc) return rc;
+  const uint32_t n = cfg->job_ids ? cfg->njob_ids : cfg->njobs;
+  memset(out, 0, sizeof(*out));
+  if (n == 0) return HA_OK;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+
+  std::vector<uint32_t> order(n);
+  for (uint32_t i = 0; i < n; i++) order[i] = cfg->job_ids ? cfg->job_ids[i] : i;
+  for (uint32_t i = 0; i < n; i++)
+    if (order[i] >= cfg->njobs) return HA_EINVAL;  // results has 2*njobs words
+
+  uint32_t *d_order = nullptr;
+  ServeDev *d_dev = nullptr;
+  ServeCtl *h_ctl = nullptr, *d_ctl = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(d_order);
+    cudaFree(d_dev);
+    if (h_ctl) cudaFreeHost(h_ctl);
+  };
+  if (cudaMalloc(&d_order, n * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&d_dev, sizeof(ServeDev)) != cudaSuccess ||
+      cudaHostAlloc(&h_ctl, sizeof(ServeCtl), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&d_ctl, h_ctl, 0) != cudaSuccess ||
+      cudaMemcpy(d_order, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemset(d_dev, 0, sizeof(ServeDev)) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    return HA_ECUDA;
+  }
+  __atomic_store_n(&h_ctl->released, 0u, __ATOMIC_RELEASE);
+  __atomic_store_n(&h_ctl->ended, 0u, __ATOMIC_RELEASE);
+
+  // Poisson arrival times (seconds from the start)
+  std::mt19937_64 rng(cfg->seed * 0x9E3779B97F4A7C15ull + 1);
+  std::exponential_distribution<double> gap(cfg->lambda);
+  std::vector<double> arrive(n);
+  double t = 0;
+  for (uint32_t i = 0; i < n; i++) arrive[i] = (t += gap(rng));
+
+  int dev = 0, nsm = 0, fit = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, ha_serve_k, (int)cfg->cta_threads, 0) !=
+          cudaSuccess ||
+      fit <= 0) {
+    cleanup();
+    return HA_ECUDA;
+  }
+  const uint32_t per_sm =
+      cfg->ctas_per_sm && cfg->ctas_per_sm < (uint32_t)fit ? cfg->ctas_per_sm : (uint32_t)fit;
+
+  ServeParams P;
+  P.order = d_order;
+  P.norder = n;
+  P.seed = cfg->seed;
+  P.block_bytes = cfg->block_bytes;
+  P.log_min = logf((float)cfg->min_len);
+  P.log_span = logf((float)cfg->max_len) - P.log_min;
+  P.mean_life = (float)cfg->mean_life;
+  P.grow_min = cfg->grow_min;
+  P.grow_span = cfg->grow_max - cfg->grow_min + 1;
+  P.live_limit = (unsigned long long)(cfg->occupancy_limit * (double)st.pool_bytes) /
+                 cfg->block_bytes;
+  P.results = reinterpret_cast<unsigned long long *>(cfg->results);
+  P.ctl = d_ctl;
+  P.dev = d_dev;
+
+  ha_serve_k<<<nsm * per_sm, cfg->cta_threads, 0, s>>>(P);
+  if (cudaGetLastError() != cudaSuccess) {
+    cleanup();
+    return HA_ECUDA;
+  }
+  // release jobs at their arrival times
+  const auto t0 = std::chrono::steady_clock::now();
+  uint32_t released = 0;
+  while (released < n) {
+    const double now =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    uint32_t r = released;
+    while (r < n && arrive[r] <= now) r++;
+    if (r != released) {
+      released = r;
+      __atomic_store_n(&h_ctl->released, released, __ATOMIC_RELEASE);
+    }
+  }
+  __atomic_store_n(&h_ctl->ended, 1u, __ATOMIC_RELEASE);
+  const cudaError_t e = cudaStreamSynchronize(s);
+  const double secs =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  ServeDev hd;
+  if (e != cudaSuccess || cudaMemcpy(&hd, d_dev, sizeof(hd), cudaMemcpyDeviceToHost) !=
+                              cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    return HA_ECUDA;
+  }
+  out->seconds = secs;
+  out->cycles_per_ns = hd.nanos ? (double)hd.cycles / (double)hd.nanos : 0;
+  out->jobs_done = hd.jobs_done;
+  out->allocs = hd.allocs;
+  out->alloc_failures = hd.failures;
+  out->refusals = hd.refusals;
+  out->peak_live_blocks = hd.peak_live;
+  out->timeouts = hd.timeouts;
+  memcpy(out->hist, hd.hist, sizeof(hd.hist));
+  out->p50_cycles = percentile(hd.hist, 0.50);
+  out->p99_cycles = percentile(hd.hist, 0.99);
+  for (int i = HA_SERVE_HIST - 1; i >= 0; i--)
+    if (hd.hist[i]) {
+      out->max_cycles = bucket_value(i + 1);
+      break;
+    }
+  cleanup();
+  return HA_OK;
+}

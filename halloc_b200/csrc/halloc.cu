@@ -76,6 +76,8 @@ struct HostDev {
 };
 constexpr int kMaxDevices = 64;
 HostDev g_dev[kMaxDevices];
+// hash-step scale for the next init, in percent (100 = the reference rule)
+uint32_t g_hash_scale_pct = 100;
 
 #define HA_CK(call)                                   \
   do {                                                \
@@ -127,7 +129,10 @@ bool build_classes(ha::Class *cls, uint32_t sb_bytes, const ha_opts_c &o) {
     c.chunk_enc = chunk_enc(cbytes);
     c.ncib = block / cbytes;
     c.nchunks = nblocks * c.ncib;
-    uint32_t p = prime_below(nblocks / 256 + nblocks / 64, nblocks);
+    uint64_t span = (uint64_t)(nblocks / 256 + nblocks / 64) * g_hash_scale_pct / 100;
+    if (span < 4) span = 4;
+    if (span > nblocks) span = nblocks;
+    uint32_t p = prime_below((uint32_t)span, nblocks);
     if (!p) return false;
     c.hash_step = c.ncib * p;
     c.roomy = (uint32_t)(o.roomy_fraction * c.nchunks);
@@ -507,6 +512,12 @@ extern "C" int ha_dump_state_c(const ha_state_dump_t *d) {
   if (d->bits) HA_CK(cudaMemcpy(d->bits, h->meta, bit_words * 4, cudaMemcpyDeviceToHost));
   if (d->nibbles)
     HA_CK(cudaMemcpy(d->nibbles, h->meta + bit_words, nib_words * 4, cudaMemcpyDeviceToHost));
+  return HA_OK;
+}
+
+extern "C" int ha_set_hash_scale_c(uint32_t percent) {
+  if (percent < 10 || percent > 1000) return HA_EINVAL;
+  g_hash_scale_pct = percent;
   return HA_OK;
 }
 

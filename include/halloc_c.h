@@ -107,6 +107,13 @@ int ha_dump_state_c(const ha_state_dump_t *out);
    launched on `stream` (an access-policy window over the metadata). */
 int ha_l2_persist_c(void *stream);
 
+/* Tuning knob, applied by the next init on this process: the probe hash
+   step of each size class is ncib x (largest prime below span) with span =
+   (nblocks/256 + nblocks/64) x percent / 100.  100 (the default) is the
+   reference's rule (halloc src/halloc.cu:384-385) and the only setting
+   whose addresses match it; the autotuner may pick another. 10..1000. */
+int ha_set_hash_scale_c(uint32_t percent);
+
 /* Test hook for failure detection: sets the head-replacement lock of size
    class `size_id` to `held` (1 = held by a holder that never releases it,
    0 = free).  A hamalloc that then needs a new head for that size waits
@@ -193,6 +200,117 @@ int ha_phase_run_c(uint32_t nthreads, uint32_t nslots, uint32_t seed,
                    uint64_t target_filled, uint32_t max_rounds,
                    const uint32_t *size_set, uint32_t nsizes, void **slots,
                    uint32_t *slot_sz, uint64_t *acc, ha_phase_result_t *res,
+                   void *stream);
+
+/* ---- batched workload -------------------------------------------- */
+
+/* A stream of allocation batches.  Step s (0 <= s <= nbatch) first frees
+   the requests listed for it, then (s < nbatch) allocates the requests of
+   batch s; step nbatch frees whatever is still live.  Each block carries
+   its request id in its first 8 bytes, checked when it is freed. */
+typedef struct ha_batch_plan_t {
+  uint32_t nbatch;
+  uint32_t nreq;
+  const uint32_t *req_size;      /* device, nreq: bytes of request r */
+  uint64_t *req_ptr;             /* device, nreq: block of request r */
+  const uint32_t *free_ids;      /* device, nreq: request ids by free step */
+  const uint32_t *h_batch_start; /* host, nbatch+1: batch b = requests
+                                    [h_batch_start[b], h_batch_start[b+1]) */
+  const uint32_t *h_free_start;  /* host, nbatch+2: step s frees
+                                    free_ids[h_free_start[s] .. [s+1]) */
+  uint64_t *acc; /* device, 8 words: [0] failed allocations, [1] id
+                    mismatches, [2] sum of freed request ids, [3]
+                    allocations, [4] frees, [5] dependency-wait timeouts */
+} ha_batch_plan_t;
+
+/* Plain form: two launches per step (free kernel, malloc kernel) on
+   `stream`, `block` threads per block; clears acc first.  No counterpart
+   in the reference (its benchmarks launch one kernel per phase). */
+int ha_batched_plain_c(const ha_batch_plan_t *plan, uint32_t block, void *stream);
+
+/* Persistent form: ONE kernel whose resident blocks take tasks (chunks of
+   task_items requests) from a queue in step order; a free task waits
+   (bounded) until every allocation task of the earlier batches has
+   finished.  `block` threads per block ("request group"), ctas_per_sm
+   blocks per SM (0 = as many as fit).  use_graph != 0 captures
+   [clear acc, reset queue, kernel] in a CUDA graph once, replayed by each
+   ha_batched_launch_c.  Returns an opaque handle in *out. */
+int ha_batched_prepare_c(const ha_batch_plan_t *plan, uint32_t block,
+                         uint32_t ctas_per_sm, uint32_t task_items,
+                         int use_graph, void **out);
+int ha_batched_launch_c(void *handle, void *stream);
+int ha_batched_release_c(void *handle);
+
+/* ---- random-graph build ------------------------------------------- */
+
+/* Builds a random graph on n vertices, one device thread per vertex.
+   Vertex u's out-degree is the number of entries of cdf[0..ncdf) (an
+   increasing table of 32-bit thresholds of the degree distribution) that
+   are <= mix32(u ^ seed); its k-th neighbour is
+   mix32(mix32(u ^ seed ^ 0xABCDEF01) + k * 0x9E3779B9) mod n, with mix32
+   the "lowbias32" finaliser.  The neighbours go into an int32 array from
+   hamalloc that starts at capacity 2 and doubles (malloc new, copy, hafree
+   old); arr[u] receives the array and deg[u] its length.  acc (3 device
+   words, cleared): failed allocations, doublings, edges.  Replaces
+   random_graph_build_k (halloc samples/random-graph/random-graph.cu:
+   165-181), which built linked lists. */
+int ha_graph_build_c(uint32_t n, uint32_t seed, const uint32_t *cdf,
+                     uint32_t ncdf, uint64_t *arr, uint32_t *deg,
+                     uint64_t *acc, void *stream);
+
+/* Copies every vertex's array to cols[offsets[u] ...] (a CSR, offsets =
+   exclusive prefix sum of deg) and hafree's it. */
+int ha_graph_gather_c(uint32_t n, uint64_t *arr, const uint32_t *deg,
+                      const uint64_t *offsets, uint32_t *cols, void *stream);
+
+/* ---- serving loop ------------------------------------------------ */
+
+/* A host-fed stream of jobs served by continuous batching.  Job j (an id;
+   every parameter derives from a hash of (seed, j)) has a target of
+   ceil(L/block_bytes) blocks, L log-uniform in [min_len, max_len]; on each
+   step it gains grow_min..grow_max blocks (hamalloc(block_bytes) each,
+   linked through their first 8 bytes, the next 4 bytes holding a hashed
+   value) until the target, and it ends after an Exp(mean_life) number of
+   steps: its blocks are read back (result = number of blocks and sum of the
+   values) and hafree'd.  Arrivals are Poisson with rate `lambda` jobs/s:
+   a host thread releases job ids at their arrival times through a mapped
+   host counter.  One persistent kernel serves them: each block of
+   cta_threads threads owns that many job slots, claims released jobs for
+   its empty slots while the slab pool's occupancy is at most
+   occupancy_limit (otherwise the admission is refused and retried), steps
+   its jobs, and leaves once the stream has ended and its slots are empty.
+   Every hamalloc's latency (clock64 cycles) goes into a log-linear
+   histogram.  With job_ids != NULL only those jobs (in that order) are
+   released, e.g. to serve one job alone.  No counterpart in the
+   reference. */
+typedef struct ha_serve_cfg_t {
+  uint32_t njobs;          /* jobs in the stream (ids 0..njobs-1) */
+  uint32_t seed;
+  double lambda;           /* arrival rate, jobs per second */
+  double occupancy_limit;  /* admission gate on slab-pool occupancy */
+  double mean_life;        /* mean job lifetime in steps */
+  uint32_t block_bytes;    /* bytes per block (256) */
+  uint32_t min_len, max_len;
+  uint32_t grow_min, grow_max;
+  uint32_t cta_threads;    /* slots per persistent block */
+  uint32_t ctas_per_sm;    /* 0 = as many as fit */
+  const uint32_t *job_ids; /* host, optional: the ids to release, in order */
+  uint32_t njob_ids;
+  uint64_t *results;       /* device, 2 words per job id: blocks, value sum */
+} ha_serve_cfg_t;
+
+#define HA_SERVE_HIST 1024 /* histogram buckets: 16 per power of two */
+
+typedef struct ha_serve_result_t {
+  double seconds;          /* first release to kernel completion, wall */
+  double cycles_per_ns;    /* SM clock seen by the kernel */
+  uint64_t jobs_done, allocs, alloc_failures, refusals, peak_live_blocks;
+  uint64_t timeouts;       /* idle waits that gave up */
+  double p50_cycles, p99_cycles, max_cycles;
+  uint64_t hist[HA_SERVE_HIST];
+} ha_serve_result_t;
+
+int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out,
                    void *stream);
 
 /* Replays a trace on ONE device thread: op >= 0 is hamalloc(op);

@@ -1,0 +1,63 @@
+"""Serving loop: a host-fed Poisson stream of jobs served by continuous
+batching in one persistent kernel.  Every job completes, nothing fails,
+each block's payload survives to the job's end (the value sum equals the
+host recomputation), the pool is empty afterwards, and a job's result is
+the same served alone as in the mix."""
+import numpy as np
+import pytest
+
+from oracle.phase import mix32
+from tests.helpers import allocator
+
+pytestmark = pytest.mark.gpu
+
+CFG = dict(lam=2e6, seed=11, mean_life=20.0, min_len=64, max_len=64 << 10)
+
+
+def value_sums(ids: np.ndarray, blocks: np.ndarray) -> np.ndarray:
+    """Sum over k < blocks of mix32(id * 0x27D4EB2F + k), per job."""
+    out = np.zeros(len(ids), np.uint64)
+    for i, (j, b) in enumerate(zip(ids, blocks)):
+        k = np.arange(int(b), dtype=np.uint32)
+        out[i] = mix32(np.uint32((int(j) * 0x27D4EB2F) & 0xFFFFFFFF) + k).astype(np.uint64).sum()
+    return out
+
+
+def test_serving_stream_and_alone_vs_mix(torch_cuda):
+    import halloc_b200 as H
+    torch = torch_cuda
+    n = 3000
+    with allocator(memory=1 << 30):
+        res = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+        r = H.serve_run(res, n, **CFG)
+        assert r["jobs_done"] == n and r["alloc_failures"] == 0 and r["timeouts"] == 0
+        assert r["allocs"] > n and r["p99_cycles"] >= r["p50_cycles"] > 0
+        assert int(r["hist"].sum()) == r["allocs"]
+        mix = res.view(-1, 2).cpu().numpy().astype(np.uint64)
+        assert (mix[:, 0] >= 1).all()
+        ids = np.arange(n)
+        assert np.array_equal(mix[:, 1], value_sums(ids, mix[:, 0]))
+        st = H.stats()
+        assert st["used_chunks"] == 0 and st["status"] == 0
+        # the same jobs, each served alone
+        for j in (0, 7, 1234, n - 1):
+            alone = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+            r1 = H.serve_run(alone, n, job_ids=[j], **CFG)
+            assert r1["jobs_done"] == 1
+            a = alone.view(-1, 2)[j].cpu().numpy().astype(np.uint64)
+            assert np.array_equal(a, mix[j]), j
+        assert H.stats()["used_chunks"] == 0
+
+
+def test_admission_gate_refuses_and_recovers(torch_cuda):
+    """With a tiny occupancy limit most admissions are refused at first;
+    jobs still all complete once memory frees up."""
+    import halloc_b200 as H
+    torch = torch_cuda
+    n = 800
+    with allocator(memory=1 << 30):
+        res = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+        r = H.serve_run(res, n, occupancy_limit=0.0005, **CFG)
+        assert r["refusals"] > 0
+        assert r["jobs_done"] == n and r["alloc_failures"] == 0 and r["timeouts"] == 0
+        assert H.stats()["used_chunks"] == 0 and H.status() == 0
