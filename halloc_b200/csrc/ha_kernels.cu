@@ -356,6 +356,53 @@ __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uin
   block_add2(nfree, late, acc + 4, acc + 5);
 }
 
+// ---- batched persistent form that allocates nothing ----------------------------
+//
+// Some callers cannot call cudaMalloc: code that has handed all device
+// memory to its own pool (cudaMalloc would fail), and latency-bound serving
+// loops that must not call cudaMalloc/cudaFree because those calls
+// synchronise the device and stall every other stream.  For them the
+// persistent form below keeps its scratch -- the task table, the per-batch
+// task counts, the queue and completion counters, and a copy of the step
+// offsets -- in one fixed array in device memory instead.  Every GPU that
+// loads this library holds the array (about 1 MiB) until the process exits.
+
+constexpr uint32_t kNoAllocMaxTasks = 65536;
+constexpr uint32_t kNoAllocMaxBatches = 1024;
+constexpr size_t kNaTasksOff = 0;
+constexpr size_t kNaBtasksOff = kNaTasksOff + sizeof(BatchTask) * kNoAllocMaxTasks;
+constexpr size_t kNaCtlOff = kNaBtasksOff + 4 * 1280;
+constexpr size_t kNaBatchStartOff = kNaCtlOff + 4 * 1280;
+constexpr size_t kNaFreeStartOff = kNaBatchStartOff + 4 * 1280;
+constexpr size_t kNoAllocScratchBytes = kNaFreeStartOff + 4 * 1280;
+static_assert(kNoAllocMaxBatches + 2 <= 1280, "scratch regions hold nbatch + 2 words");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Builds the task table of ha_batched_prepare_c in the scratch array from the
+// step offsets copied there, and clears the queue and completion counters.
+__global__ void ha_noalloc_tasks_k(unsigned char *scratch, uint32_t nbatch, uint32_t items) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  BatchTask *tasks = reinterpret_cast<BatchTask *>(scratch + kNaTasksOff);
+  uint32_t *btasks = reinterpret_cast<uint32_t *>(scratch + kNaBtasksOff);
+  unsigned int *ctl = reinterpret_cast<unsigned int *>(scratch + kNaCtlOff);
+  const uint32_t *bs = reinterpret_cast<const uint32_t *>(scratch + kNaBatchStartOff);
+  const uint32_t *fs = reinterpret_cast<const uint32_t *>(scratch + kNaFreeStartOff);
+  uint32_t n = 0;
+  for (uint32_t st = 0; st <= nbatch; st++) {
+    for (uint32_t k = fs[st]; k < fs[st + 1]; k += items)
+      tasks[n++] = {k, min(k + items, fs[st + 1]), st, 1u};
+    ctl[1 + st] = 0;
+    if (st == nbatch) break;
+    btasks[st] = 0;
+    for (uint32_t r = bs[st]; r < bs[st + 1]; r += items) {
+      tasks[n++] = {r, min(r + items, bs[st + 1]), st, 0u};
+      btasks[st]++;
+    }
+  }
+  ctl[0] = 0;
+}
+
 // ---- random-graph build -----------------------------------------------------
 //
 // Vertex u draws its out-degree d from a Poisson CDF given as 32-bit
@@ -766,6 +813,66 @@ extern "C" int ha_graph_gather_c(uint32_t n, uint64_t *arr, const uint32_t *deg,
   ha_graph_gather_k<<<blocks_for(n, 128), 128, 0, as_stream(stream)>>>(
       n, reinterpret_cast<unsigned long long *>(arr), deg,
       reinterpret_cast<const unsigned long long *>(offsets), cols);
+  return launch_status();
+}
+
+namespace {
+constexpr int kNoAllocDevices = 64;
+unsigned char *g_noalloc_addr[kNoAllocDevices];  // scratch address per device
+}  // namespace
+
+extern "C" int ha_batched_run_noalloc_c(const ha_batch_plan_t *plan, uint32_t block,
+                                        uint32_t ctas_per_sm, uint32_t task_items,
+                                        void *stream) {
+  if (!plan || !plan->acc || !plan->h_batch_start || !plan->h_free_start || block == 0 ||
+      block > 1024 || block % 32 || task_items == 0)
+    return HA_EINVAL;
+  if (plan->nbatch > kNoAllocMaxBatches) return HA_ERANGE;
+  uint64_t ntasks = 0;
+  for (uint32_t st = 0; st <= plan->nbatch; st++) {
+    ntasks += (plan->h_free_start[st + 1] - plan->h_free_start[st] + (uint64_t)task_items - 1) /
+              task_items;
+    if (st < plan->nbatch)
+      ntasks += (plan->h_batch_start[st + 1] - plan->h_batch_start[st] +
+                 (uint64_t)task_items - 1) / task_items;
+  }
+  if (ntasks > kNoAllocMaxTasks) return HA_ERANGE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocDevices) return HA_ECUDA;
+  if (!g_noalloc_addr[dev]) {
+    // once per device: the device address of the scratch array (in host code
+    // the symbol names a host-side stand-in, not device memory)
+    unsigned char *p = nullptr;
+    if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return HA_ECUDA;
+    }
+    g_noalloc_addr[dev] = p;
+  }
+  unsigned char *scratch = g_noalloc_addr[dev];
+  int nsm = 0, fit = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, ha_bpersist_k, (int)block, 0) !=
+          cudaSuccess || fit <= 0)
+    return HA_ECUDA;
+  const uint32_t grid =
+      (uint32_t)nsm * (ctas_per_sm && ctas_per_sm < (uint32_t)fit ? ctas_per_sm : fit);
+  cudaStream_t s = as_stream(stream);
+  unsigned long long *acc = reinterpret_cast<unsigned long long *>(plan->acc);
+  if (cudaMemcpyAsync(scratch + kNaBatchStartOff, plan->h_batch_start,
+                      (plan->nbatch + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(scratch + kNaFreeStartOff, plan->h_free_start,
+                      (plan->nbatch + 2) * sizeof(uint32_t), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemsetAsync(acc, 0, 8 * sizeof(uint64_t), s) != cudaSuccess)
+    return HA_ECUDA;
+  ha_noalloc_tasks_k<<<1, 1, 0, s>>>(scratch, plan->nbatch, task_items);
+  ha_bpersist_k<<<grid, block, 0, s>>>(
+      reinterpret_cast<const BatchTask *>(scratch + kNaTasksOff), (uint32_t)ntasks,
+      reinterpret_cast<const uint32_t *>(scratch + kNaBtasksOff), plan->req_size,
+      reinterpret_cast<unsigned long long *>(plan->req_ptr), plan->free_ids,
+      reinterpret_cast<unsigned int *>(scratch + kNaCtlOff), acc);
   return launch_status();
 }
 

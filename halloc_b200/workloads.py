@@ -78,6 +78,9 @@ class BatchedRunner:
                  [ctypes.POINTER(_CPlan), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                   ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
                 ("ha_batched_launch_c", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+                ("ha_batched_run_noalloc_c", ctypes.c_int,
+                 [ctypes.POINTER(_CPlan), ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                  ctypes.c_void_p]),
                 ("ha_batched_release_c", ctypes.c_int, [ctypes.c_void_p])):
             f = getattr(lib, name)
             f.restype, f.argtypes = res, args
@@ -106,6 +109,14 @@ class BatchedRunner:
                "ha_batched_prepare_c")
         self.handles.append(h)
         return h
+
+    def run_noalloc(self, block: int = 256, ctas_per_sm: int = 0, task_items: int = 2048,
+                    stream=None) -> int:
+        """The persistent form through ha_batched_run_noalloc_c, which
+        allocates nothing (for callers that cannot call cudaMalloc).  Returns
+        the C return code (HA_ERANGE for a plan beyond its fixed limits)."""
+        return self.lib.ha_batched_run_noalloc_c(ctypes.byref(self.c), block, ctas_per_sm,
+                                                 task_items, _stream(stream))
 
     def launch(self, handle, stream=None) -> None:
         _check(self.lib.ha_batched_launch_c(handle, _stream(stream)), "ha_batched_launch_c")

@@ -241,6 +241,23 @@ int ha_batched_prepare_c(const ha_batch_plan_t *plan, uint32_t block,
 int ha_batched_launch_c(void *handle, void *stream);
 int ha_batched_release_c(void *handle);
 
+/* The persistent form for callers that cannot call cudaMalloc -- code that
+   has given all device memory to its own pool, or a latency-bound serving
+   loop that must not call cudaMalloc/cudaFree because they synchronise the
+   device.  It allocates nothing: the task table and counters live in one
+   fixed array of device memory that every GPU loading this library holds
+   until exit (about 1 MiB).  Limits: at most 65,536 tasks (ceil of each
+   step's frees and of each batch's requests over task_items, summed) and
+   1,024 batches, else HA_ERANGE.  The first call on a device looks up the
+   array's device address, with that device current; make that first call
+   before any stream capture.  Each call rebuilds the table and clears the
+   counters, but all calls share the one array: calls that overlap on the
+   GPU race, so serialise them (one stream, or events).  The caller still
+   provides the plan's buffers and acc.  No counterpart in the reference. */
+int ha_batched_run_noalloc_c(const ha_batch_plan_t *plan, uint32_t block,
+                             uint32_t ctas_per_sm, uint32_t task_items,
+                             void *stream);
+
 /* ---- random-graph build ------------------------------------------- */
 
 /* Builds a random graph on n vertices, one device thread per vertex.
