@@ -4,11 +4,12 @@
 // Jobs are ids; every parameter derives from a hash of (seed, id), so a
 // job's result does not depend on what else runs beside it.  A host thread
 // releases ids at Poisson arrival times through a counter in mapped host
-// memory.  Each thread of the persistent kernel owns one job slot; a block
+// memory.  Each thread of the persistent kernel owns one job slot; a warp
 // claims released jobs for its empty slots while the slab pool is at most
 // `occupancy_limit` full, then advances every active job by one step:
 // grow by 1..32 blocks of 256 B (hamalloc, linked through the blocks), and
-// at the end of the job's lifetime read its blocks back and hafree them.
+// after the job's lifetime read its blocks back and hafree them, a bounded
+// number per step.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -30,8 +31,8 @@ struct ServeCtl {  // mapped host memory, written by the host
 };
 
 struct ServeDev {  // device memory
-  uint32_t claimed;  // next index of order[] to hand out
-  uint32_t pad;
+  uint32_t claimed;        // next index of order[] to hand out
+  uint32_t released_seen;  // largest host release count a warp has read
   unsigned long long live_blocks, peak_live;
   unsigned long long jobs_done, allocs, failures, refusals, timeouts;
   unsigned long long cycles, nanos;
@@ -94,93 +95,113 @@ __device__ __forceinline__ void job_start(Job &j, uint32_t id, const ServeParams
   j.steps = 0;
 }
 
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+
+constexpr uint32_t kDrainPerStep = 64;  // blocks a finished job frees per step
+
+// Each warp runs its own loop: claim released jobs for its empty slots
+// (while the pool is under the admission limit), then give every slot one
+// bounded step -- grow by up to grow_max blocks, or, once the job's lifetime
+// is over, read back and free up to kDrainPerStep of its blocks.  No step
+// waits for other warps.
 __global__ void __launch_bounds__(1024) ha_serve_k(ServeParams P) {
   __shared__ unsigned long long s_hist[HA_SERVE_HIST];
-  __shared__ uint32_t s_base, s_n, s_exit;
-  __shared__ uint32_t s_warp_empty[32];
   for (uint32_t i = threadIdx.x; i < HA_SERVE_HIST; i += blockDim.x) s_hist[i] = 0;
+  __syncthreads();
   const uint64_t ns0 = now_ns();
   const long long cyc0 = clock64();
+  const uint32_t lane = threadIdx.x & 31;
   Job j;
   j.id = 0xffffffffu;
+  bool draining = false;
   void *head = nullptr;
-  unsigned long long vsum = 0, my_allocs = 0, my_fail = 0, my_done = 0;
+  unsigned long long vsum = 0, my_allocs = 0, my_fail = 0, my_done = 0, my_refused = 0;
   uint64_t idle_since = 0;
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (;;) {
-    // ---- admission ------------------------------------------------------
+    // ---- admission, one claim per warp -------------------------------------
     const bool empty = j.id == 0xffffffffu;
     const uint32_t em = __ballot_sync(0xffffffffu, empty);
-    if (lane == 0) s_warp_empty[warp] = __popc(em);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t nempty = 0;
-      for (uint32_t w = 0; w < (blockDim.x + 31) / 32; w++) nempty += s_warp_empty[w];
-      uint32_t base = 0, k = 0;
-      if (nempty) {
-        if (atomicAdd(&P.dev->live_blocks, 0ull) > P.live_limit) {
-          atomicAdd(&P.dev->refusals, 1ull);
-        } else {
-          for (;;) {
-            const uint32_t c = atomicAdd(&P.dev->claimed, 0u);
-            const uint32_t r = min(ld_acquire_sys(&P.ctl->released), P.norder);
-            k = r > c ? min(nempty, r - c) : 0;
-            if (!k || atomicCAS(&P.dev->claimed, c, c + k) == c) {
-              base = c;
-              break;
-            }
+    uint32_t base = 0, k = 0;
+    if (em && lane == 0) {
+      if (ld_relaxed_u64(&P.dev->live_blocks) > P.live_limit) {
+        my_refused++;
+      } else {
+        uint32_t c = ld_relaxed_u32(&P.dev->claimed);
+        uint32_t r = min(ld_relaxed_u32(&P.dev->released_seen), P.norder);
+        if (r <= c) {  // nothing known to be claimable: look at the host counter
+          r = min(ld_acquire_sys(&P.ctl->released), P.norder);
+          if (r > c) atomicMax(&P.dev->released_seen, r);
+        }
+        while (r > c) {
+          const uint32_t want = min((uint32_t)__popc(em), r - c);
+          const uint32_t got = atomicCAS(&P.dev->claimed, c, c + want);
+          if (got == c) {
+            base = c;
+            k = want;
+            break;
           }
+          c = got;
         }
       }
-      s_base = base;
-      s_n = k;
     }
-    __syncthreads();
+    base = __shfl_sync(0xffffffffu, base, 0);
+    k = __shfl_sync(0xffffffffu, k, 0);
     if (empty) {
-      // rank of this empty slot among the block's empty slots
-      uint32_t rank = __popc(em & ((1u << lane) - 1));
-      for (uint32_t w = 0; w < warp; w++) rank += s_warp_empty[w];
-      if (rank < s_n) {
-        job_start(j, P.order[s_base + rank], P);
+      const uint32_t rank = __popc(em & ((1u << lane) - 1));
+      if (rank < k) {
+        job_start(j, P.order[base + rank], P);
+        draining = false;
         head = nullptr;
         vsum = 0;
       }
     }
-    // ---- one step of every active job -------------------------------------
+    // ---- one bounded step of this lane's job --------------------------------
     uint32_t grown = 0, freed = 0;
     if (j.id != 0xffffffffu) {
-      const uint32_t g =
-          P.grow_min + mix32(j.h + j.steps * 0x9E3779B9u) % P.grow_span;
-      for (uint32_t i = 0; i < g && j.blocks < j.target; i++) {
-        const long long t0 = clock64();
-        void *p = hamalloc(P.block_bytes);
-        const long long t1 = clock64();
-        atomicAdd(&s_hist[lat_bucket((unsigned long long)(t1 - t0))], 1ull);
-        my_allocs++;
-        if (!p) {
-          my_fail++;
-          break;
+      if (!draining) {
+        const uint32_t g =
+            P.grow_min + mix32(j.h + j.steps * 0x9E3779B9u) % P.grow_span;
+        for (uint32_t i = 0; i < g && j.blocks < j.target; i++) {
+          const long long t0 = clock64();
+          void *p = hamalloc(P.block_bytes);
+          const long long t1 = clock64();
+          atomicAdd(&s_hist[lat_bucket((unsigned long long)(t1 - t0))], 1ull);
+          my_allocs++;
+          if (!p) {
+            my_fail++;
+            break;
+          }
+          *reinterpret_cast<void **>(p) = head;
+          reinterpret_cast<uint32_t *>(p)[2] = mix32(j.id * 0x27D4EB2Fu + j.blocks);
+          head = p;
+          j.blocks++;
+          grown++;
         }
-        const uint32_t v = mix32(j.id * 0x27D4EB2Fu + j.blocks);
-        *reinterpret_cast<void **>(p) = head;
-        reinterpret_cast<uint32_t *>(p)[2] = v;
-        head = p;
-        j.blocks++;
-        grown++;
-      }
-      if (++j.steps >= j.life) {
-        for (void *p = head; p;) {
-          void *nx = *reinterpret_cast<void **>(p);
-          vsum += reinterpret_cast<const uint32_t *>(p)[2];
-          hafree(p);
-          p = nx;
+        if (++j.steps >= j.life) draining = true;
+      } else {
+        for (uint32_t i = 0; i < kDrainPerStep && head; i++) {
+          void *nx = *reinterpret_cast<void **>(head);
+          vsum += reinterpret_cast<const uint32_t *>(head)[2];
+          hafree(head);
+          head = nx;
+          freed++;
         }
-        P.results[2 * (size_t)j.id] = j.blocks;
-        P.results[2 * (size_t)j.id + 1] = vsum;
-        freed = j.blocks;
-        my_done++;
-        j.id = 0xffffffffu;
-        head = nullptr;
+        if (!head) {
+          P.results[2 * (size_t)j.id] = j.blocks;
+          P.results[2 * (size_t)j.id + 1] = vsum;
+          my_done++;
+          j.id = 0xffffffffu;
+          draining = false;
+        }
       }
     }
     // live-block count, one atomic per warp
@@ -191,13 +212,13 @@ __global__ void __launch_bounds__(1024) ha_serve_k(ServeParams P) {
           atomicAdd(&P.dev->live_blocks, (unsigned long long)delta) + (unsigned long long)delta;
       if (delta > 0) atomicMax(&P.dev->peak_live, now);
     }
-    // ---- leave when the stream has ended and the block is idle -------------
-    const uint32_t active = __syncthreads_count(j.id != 0xffffffffu);
-    if (threadIdx.x == 0) {
+    // ---- leave when the stream has ended and this warp is idle ---------------
+    const uint32_t active = __ballot_sync(0xffffffffu, j.id != 0xffffffffu);
+    if (active == 0 && k == 0) {
       uint32_t leave = 0;
-      if (active == 0 && s_n == 0) {
-        const bool ended = ld_acquire_sys(&P.ctl->ended) != 0;
-        if (ended && atomicAdd(&P.dev->claimed, 0u) >= P.norder) {
+      if (lane == 0) {
+        if (ld_acquire_sys(&P.ctl->ended) &&
+            ld_relaxed_u32(&P.dev->claimed) >= P.norder) {
           leave = 1;
         } else {
           const uint64_t t = now_ns();
@@ -206,27 +227,27 @@ __global__ void __launch_bounds__(1024) ha_serve_k(ServeParams P) {
             atomicAdd(&P.dev->timeouts, 1ull);
             leave = 1;
           } else {
-            __nanosleep(1000);
+            __nanosleep(2000);
           }
         }
-      } else {
-        idle_since = 0;
       }
-      s_exit = leave;
+      if (__shfl_sync(0xffffffffu, leave, 0)) break;
+    } else {
+      idle_since = 0;
     }
-    __syncthreads();
-    if (s_exit) break;
   }
   // ---- totals ---------------------------------------------------------------
   for (int o = 16; o > 0; o >>= 1) {
     my_allocs += __shfl_down_sync(0xffffffffu, my_allocs, o);
     my_fail += __shfl_down_sync(0xffffffffu, my_fail, o);
     my_done += __shfl_down_sync(0xffffffffu, my_done, o);
+    my_refused += __shfl_down_sync(0xffffffffu, my_refused, o);
   }
   if (lane == 0) {
     if (my_allocs) atomicAdd(&P.dev->allocs, my_allocs);
     if (my_fail) atomicAdd(&P.dev->failures, my_fail);
     if (my_done) atomicAdd(&P.dev->jobs_done, my_done);
+    if (my_refused) atomicAdd(&P.dev->refusals, my_refused);
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < HA_SERVE_HIST; i += blockDim.x)

@@ -291,11 +291,12 @@ int ha_graph_gather_c(uint32_t n, uint64_t *arr, const uint32_t *deg,
    steps: its blocks are read back (result = number of blocks and sum of the
    values) and hafree'd.  Arrivals are Poisson with rate `lambda` jobs/s:
    a host thread releases job ids at their arrival times through a mapped
-   host counter.  One persistent kernel serves them: each block of
-   cta_threads threads owns that many job slots, claims released jobs for
-   its empty slots while the slab pool's occupancy is at most
-   occupancy_limit (otherwise the admission is refused and retried), steps
-   its jobs, and leaves once the stream has ended and its slots are empty.
+   host counter.  One persistent kernel serves them: each thread owns a
+   job slot; each warp claims released jobs for its empty slots while the
+   slab pool's occupancy is at most occupancy_limit (otherwise the
+   admission is refused and retried), steps its jobs independently of other
+   warps (a finished job frees at most 64 blocks per step), and leaves once
+   the stream has ended and its slots are empty.
    Every hamalloc's latency (clock64 cycles) goes into a log-linear
    histogram.  With job_ids != NULL only those jobs (in that order) are
    released, e.g. to serve one job alone.  No counterpart in the
