@@ -293,6 +293,11 @@ def leg_main(args):
     torch.cuda.set_device(0)
     if args.leg == "phase":
         out = run_phase(torch, H, 3, hbm_peak())
+        tuned = run_phase(torch, H, 3, hbm_peak(), nheads=4)
+        out["tuned_4_heads"] = {"value": tuned["value"], "ms_per_run": tuned["ms_per_run"],
+                                "ok": tuned["ok"],
+                                "note": "4 head slabs per size (ha_set_heads_c); addresses "
+                                        "no longer follow the reference policy"}
     elif args.leg == "graph":
         out = run_graph(torch, H, 3)
     elif args.leg == "serve":
@@ -307,13 +312,15 @@ PHASE_THREADS, PHASE_SLOTS, PHASE_PERIODS, PHASE_POOL = 1 << 20, 4, 5, 1 << 30
 THR95 = int(0.95 * 2**32)
 
 
-def run_phase(torch, H, reps: int, hbm_peak_gbs: float | None) -> dict:
+def run_phase(torch, H, reps: int, hbm_peak_gbs: float | None, nheads: int = 1) -> dict:
     """Mixed-size phase workload: 1,048,576 threads x 4 slots, 1 GiB pool,
     sizes uniform over 16..256 B, 5 periods of (allocation rounds with p=0.95
     until 91 % of the slots are filled; a free round with p=0.95), then the
     rest freed; every block written with a hashed pattern and read back
-    before it is freed."""
+    before it is freed.  nheads > 1 is the tuned multi-head variant."""
+    H.set_heads(nheads)
     H.init(H.HallocOpts(memory=PHASE_POOL))
+    H.set_heads(1)
     stream = torch.cuda.current_stream()
     H.l2_persist(stream)
     n = PHASE_THREADS
@@ -437,6 +444,23 @@ def run_serve(torch, H) -> dict:
             "p99_cycles": r["p99_cycles"], "sm_ghz": cpn})
         del res
     ok &= H.status() == 0 and H.stats()["used_chunks"] == 0
+    H.shutdown()
+    # tuned variant: two head slabs per size
+    H.set_heads(2)
+    H.init(H.HallocOpts(memory=SERVE_POOL))
+    H.set_heads(1)
+    lam, njobs = SERVE_POINTS[-1]
+    res = torch.zeros(2 * njobs, dtype=torch.int64, device="cuda")
+    r = H.serve_run(res, njobs, lam, seed=7)
+    cpn = r["cycles_per_ns"] or 1.0
+    out["tuned_2_heads"] = {"lambda": lam, "jobs": njobs,
+                            "jobs_per_s": r["jobs_done"] / r["seconds"],
+                            "allocs_per_s": r["allocs"] / r["seconds"],
+                            "alloc_failures": r["alloc_failures"],
+                            "p50_ns": r["p50_cycles"] / cpn, "p99_ns": r["p99_cycles"] / cpn,
+                            "ok": r["jobs_done"] == njobs and r["timeouts"] == 0,
+                            "note": "2 head slabs per size (ha_set_heads_c)"}
+    del res
     H.shutdown()
     out["ok"] = ok
     out["config"] = ("jobs of ceil(L/256) 256-B blocks, L log-uniform 64 B..2 MiB, growing "

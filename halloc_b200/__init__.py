@@ -25,7 +25,7 @@ __all__ = [
     "clear_status", "set_wait_limit", "dump_state", "l2_persist", "malloc_batch",
     "free_batch", "phase_round", "phase_run", "graph_build", "graph_gather", "serve_run",
     "throughput", "throughput_host", "cuda_throughput", "trace",
-    "atomic_peak", "debug_set_head_lock", "set_hash_scale", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
+    "atomic_peak", "debug_set_head_lock", "set_hash_scale", "set_heads", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
 ]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -124,6 +124,7 @@ _SIGS = {
     "ha_l2_persist_c": (_int, [_vp]),
     "ha_debug_set_head_lock_c": (_int, [_u32, _u32]),
     "ha_set_hash_scale_c": (_int, [_u32]),
+    "ha_set_heads_c": (_int, [_u32]),
     "ha_serve_run_c": (_int, [ctypes.POINTER(_CServeCfg), ctypes.POINTER(_CServeResult), _vp]),
     "ha_graph_build_c": (_int, [_u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
     "ha_graph_gather_c": (_int, [_u32, _vp, _vp, _vp, _vp, _vp]),
@@ -260,6 +261,11 @@ def dump_state() -> dict:
 def set_hash_scale(percent: int) -> None:
     """Hash-step scale for the next init (100 = the reference's rule)."""
     _check(load().ha_set_hash_scale_c(percent), "ha_set_hash_scale_c")
+
+
+def set_heads(nheads: int) -> None:
+    """Head slabs per size for the next init (1 = the reference policy)."""
+    _check(load().ha_set_heads_c(nheads), "ha_set_heads_c")
 
 
 def debug_set_head_lock(size_id: int, held: bool) -> None:

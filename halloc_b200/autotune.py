@@ -1,25 +1,26 @@
 """Autotuner for the batched persistent form.
 
-Sweeps, in two stages, the slab size {2, 4, 8} MiB x busy fraction
-{0.745, 0.835, 0.91} (sparse fraction follows: 0.012 or 0.0125), then, at the
+Sweeps, in three stages, the slab size {2, 4, 8} MiB x busy fraction
+{0.745, 0.835, 0.91} (sparse fraction follows: 0.012 or 0.0125); then, at the
 best of those, the request-group size (threads per persistent block: 4, 8 or
-16 warps) x the probe hash-step scale {50, 100, 200} %.  Each point
-re-initialises the allocator, prepares the graph-captured persistent launch
-and keeps the best of `reps` timed replays.  Only settings with hash scale
-100 keep the reference's address sequence; the others are reported as tuned
-variants.
+16 warps) x the probe hash-step scale {50, 100, 200} %; then the head slabs
+per size {1, 2, 4}.  Each point re-initialises the allocator, prepares the
+graph-captured persistent launch and keeps the best of `reps` timed
+replays.  Only settings with hash scale 100 and one head keep the
+reference's address sequence; the others are reported as tuned variants.
 """
 from __future__ import annotations
 
 import itertools
 
-from . import HallocOpts, init, set_hash_scale, shutdown
+from . import HallocOpts, init, set_hash_scale, set_heads, shutdown
 from .workloads import BatchedRunner
 
 
 def _time_point(torch, runner: BatchedRunner, opts: HallocOpts, block: int, items: int,
-                hash_pct: int, reps: int) -> float:
+                hash_pct: int, reps: int, nheads: int = 1) -> float:
     set_hash_scale(hash_pct)
+    set_heads(nheads)
     init(opts)
     try:
         h = runner.prepare(block=block, task_items=items, graph=True)
@@ -42,6 +43,7 @@ def _time_point(torch, runner: BatchedRunner, opts: HallocOpts, block: int, item
     finally:
         shutdown()
         set_hash_scale(100)
+        set_heads(1)
 
 
 def autotune(torch, runner: BatchedRunner, memory: int, halloc_fraction: float,
@@ -63,5 +65,14 @@ def autotune(torch, runner: BatchedRunner, memory: int, halloc_fraction: float,
                          task_items, hp, reps)
         points.append({"sb_sz_sh": best["sb_sz_sh"], "busy": best["busy"], "block": block,
                        "hash_pct": hp, "ms": ms})
+    best = min(points, key=lambda p: p["ms"])
+    for nh in (2, 4):
+        ms = _time_point(torch, runner, opts(best["sb_sz_sh"], best["busy"]), best["block"],
+                         task_items, best["hash_pct"], reps, nh)
+        points.append({"sb_sz_sh": best["sb_sz_sh"], "busy": best["busy"],
+                       "block": best["block"], "hash_pct": best["hash_pct"], "nheads": nh,
+                       "ms": ms})
+    for p in points:
+        p.setdefault("nheads", 1)
     best = min(points, key=lambda p: p["ms"])
     return {"best": best, "points": points}

@@ -51,6 +51,11 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
 }
+__device__ __forceinline__ uint32_t sm_id() {
+  uint32_t v;
+  asm("mov.u32 %0, %%smid;" : "=r"(v));
+  return v;
+}
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -448,16 +453,18 @@ __device__ __noinline__ uint32_t find_slab(uint32_t sid) {
 // slab is prefetched right away.  One lane per warp calls this.  A caller
 // that loses the race for the size's lock waits (bounded) until the head
 // changes or the lock is released (halloc src/slab.cuh:378-445).
-__device__ __noinline__ uint32_t replace_head(uint32_t sid) {
-  uint32_t *head = &g_st.head[sid];
-  uint32_t *hlock = &g_st.head_lock[sid * kTicketStride];
+__device__ __noinline__ uint32_t replace_head(uint32_t hs) {
+  // hs = ihead * kNSizes + size id
+  const uint32_t sid = hs % kNSizes;
+  uint32_t *head = &g_st.head[hs];
+  uint32_t *hlock = &g_st.head_lock[hs * kTicketStride];
   uint32_t seen = ld_relaxed(head);
   if (try_lock(hlock)) {
     uint32_t cur = ld_relaxed(head);
     uint32_t next;
     if (cur == kNone || used_of(cur) >= load_class(sid).busy) {
-      next = ld_relaxed(&g_st.cached[sid]);
-      st_relaxed(&g_st.cached[sid], kNone);
+      next = ld_relaxed(&g_st.cached[hs]);
+      st_relaxed(&g_st.cached[hs], kNone);
       if (next == kNone) next = find_slab(sid);
       if (next != kNone) {
         st_release(head, next);
@@ -468,7 +475,7 @@ __device__ __noinline__ uint32_t replace_head(uint32_t sid) {
             unlock(&g_st.sb_lock[cur]);
           }
         }
-        st_relaxed(&g_st.cached[sid], find_slab(sid));
+        st_relaxed(&g_st.cached[hs], find_slab(sid));
       }
     } else {
       next = ld_relaxed(head);
@@ -526,18 +533,56 @@ __device__ __forceinline__ uint32_t next_probe(uint32_t first, uint32_t round, u
 // src/slab.cuh:469-498): tries `pos` as try number `round`, then the next
 // positions, until a block is reserved (true), the slab count reads busy at
 // an odd try, or the 32-try round ends (false).  Per lane, no warp ops.
+//
+// Look-ahead: the bit words of the next kLookahead positions and the slab
+// count are read together (one round trip), and atom.or is issued only at
+// positions whose word shows the block free.  For a thread running alone
+// this makes exactly the reference's decisions -- a loaded word is what its
+// atomicOr would have seen, a partly taken block is left unchanged by the
+// reference's OR-and-roll-back, and the count cannot change during the
+// call -- so addresses, try numbers and give-ups are identical.  Under
+// concurrency a stale word only costs one more try.
+constexpr uint32_t kLookahead = 8;
 __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t mn, uint64_t mh,
                                            uint32_t first, uint32_t block, uint32_t &pos,
                                            uint32_t &round) {
   uint32_t *bits = bits_of(sb);
   for (;;) {
-    const uint32_t mask = block << (pos & 31);
-    const uint32_t old = atom_or(&bits[pos >> 5], mask);
-    if (!(old & mask)) return true;
-    if (~old & mask) red_and(&bits[pos >> 5], ~mask | (old & mask));
-    if (round % kCountCheck == kCountCheck - 1 && used_of(sb) >= c.busy) return false;
-    pos = next_probe(first, round, c.ncib, c.nchunks, mn, c.hash_step, mh);
-    if (++round % kTriesPerRound >= kTriesPerRound - 1) return false;
+    uint32_t pp[kLookahead], ww[kLookahead];
+    pp[0] = pos;
+#pragma unroll
+    for (uint32_t i = 1; i < kLookahead; i++)
+      pp[i] = next_probe(first, round + i - 1, c.ncib, c.nchunks, mn, c.hash_step, mh);
+#pragma unroll
+    for (uint32_t i = 0; i < kLookahead; i++) ww[i] = ld_relaxed(&bits[pp[i] >> 5]);
+    const uint32_t count = used_of(sb);
+#pragma unroll
+    for (uint32_t i = 0; i < kLookahead; i++) {
+      const uint32_t r = round + i;  // try number of position pp[i]
+      const uint32_t mask = block << (pp[i] & 31);
+      if (!(ww[i] & mask)) {
+        const uint32_t old = atom_or(&bits[pp[i] >> 5], mask);
+        if (!(old & mask)) {
+          pos = pp[i];
+          round = r;
+          return true;
+        }
+        if (~old & mask) red_and(&bits[pp[i] >> 5], ~mask | (old & mask));
+      }
+      // try r failed
+      if (r % kCountCheck == kCountCheck - 1 && count >= c.busy) {
+        pos = pp[i];
+        round = r;
+        return false;
+      }
+      if ((r + 1) % kTriesPerRound >= kTriesPerRound - 1) {
+        pos = pp[i];
+        round = r + 1;
+        return false;
+      }
+    }
+    pos = next_probe(first, round + kLookahead - 1, c.ncib, c.nchunks, mn, c.hash_step, mh);
+    round += kLookahead;
   }
 }
 
@@ -583,11 +628,12 @@ constexpr uint32_t kMidRound = 4;  // continue the current probe call at pos
 // src/slab.cuh:453-535), for the whole warp `warp`: new head slabs for the
 // lanes that need one (one lane per size at a time), then further probe
 // calls for lanes still without a block.  Every lane of `warp` calls it.
-__device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t nbytes, uint32_t ticket,
-                                          uint32_t sb, uint32_t pos, uint32_t round,
-                                          uint32_t flags, void *p) {
+__device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hbase, uint32_t nbytes,
+                                          uint32_t ticket, uint32_t sb, uint32_t pos,
+                                          uint32_t round, uint32_t flags, void *p) {
   const uint32_t me = lane_id();
   const uint32_t sid = size_class(nbytes);
+  const uint32_t hs = hbase + sid;  // this lane's (head, size) slot
   const Class c = load_class(sid);
   const uint4 mm = __ldg(&g_mod[sid]);
   const uint64_t mn = mod_magic(mm.x, mm.y), mh = mod_magic(mm.z, mm.w);
@@ -602,7 +648,7 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t nbytes, uint32
       const uint32_t lead = __ffs(nmask) - 1;
       const uint32_t lsid = __shfl_sync(warp, sid, lead);
       uint32_t nsb = 0;
-      if (me == lead) nsb = replace_head(sid);
+      if (me == lead) nsb = replace_head(hs);
       nsb = __shfl_sync(warp, nsb, lead);
       if (need_head && sid == lsid) {
         sb = nsb;
@@ -655,7 +701,9 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
   const uint32_t sid = size_class(nbytes);
   const uint4 ca = __ldg(reinterpret_cast<const uint4 *>(&g_cls[sid]));
   const uint32_t nchunks = ca.x, enc = ca.y, cid = ca.z, ncib = ca.w;
-  uint32_t sb = ld_relaxed(&g_st.head[sid]);
+  // head slab set of this SM (always 0 with the reference's single head)
+  const uint32_t hbase = (sm_id() & (c_cfg.nheads - 1)) * kNSizes;
+  uint32_t sb = ld_relaxed(&g_st.head[hbase + sid]);
 
   // ticket: consecutive values for lanes of one size, in lane order
   uint32_t ticket;
@@ -663,7 +711,8 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
     const uint32_t grp = __match_any_sync(warp, sid);
     const uint32_t lead = __ffs(grp) - 1;
     uint32_t base = 0;
-    if (lane_id() == lead) base = atom_add(&g_st.ticket[sid * kTicketStride], __popc(grp));
+    if (lane_id() == lead)
+      base = atom_add(&g_st.ticket[(hbase + sid) * kTicketStride], __popc(grp));
     base = __shfl_sync(grp, base, lead);
     ticket = base + __popc(grp & lanemask_lt());
   }
@@ -702,7 +751,8 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
       flags = kWant | kNeedHead;
     }
   }
-  if (__any_sync(warp, flags != 0)) p = malloc_slow(warp, nbytes, ticket, sb, pos, round, flags, p);
+  if (__any_sync(warp, flags != 0))
+    p = malloc_slow(warp, hbase, nbytes, ticket, sb, pos, round, flags, p);
   return p;
 }
 

@@ -43,10 +43,13 @@ __device__ __forceinline__ void store16(void *p, uint4 v) {
     q[1] = make_uint2(v.z, v.w);
   }
 }
+// The read-back is a real load (ld.global.ca: cacheable in L1, never folded
+// into the preceding store by the compiler); a thread reading its own write
+// always sees it.
 __device__ __forceinline__ uint4 load16(const void *p) {
-  if (((uintptr_t)p & 15u) == 0) return __ldcg(reinterpret_cast<const uint4 *>(p));
-  const uint2 a = __ldcg(reinterpret_cast<const uint2 *>(p));
-  const uint2 b = __ldcg(reinterpret_cast<const uint2 *>(p) + 1);
+  if (((uintptr_t)p & 15u) == 0) return __ldca(reinterpret_cast<const uint4 *>(p));
+  const uint2 a = __ldca(reinterpret_cast<const uint2 *>(p));
+  const uint2 b = __ldca(reinterpret_cast<const uint2 *>(p) + 1);
   return make_uint4(a.x, a.y, b.x, b.y);
 }
 

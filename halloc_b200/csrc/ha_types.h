@@ -44,6 +44,7 @@ constexpr uint32_t kNSets = kSetBusy + kNSizes;
 constexpr uint32_t kTicketStride = 32;  // one 128-B line per size's ticket / lock
 constexpr uint32_t kCtrStride = 8;      // one 32-B sector per slab counter
 constexpr uint32_t kMaxRounds = 1u << 16;  // outer-loop bound of one hamalloc
+constexpr uint32_t kMaxHeads = 8;          // head slabs per size (1 = the reference policy)
 constexpr uint32_t kDefaultWaitUs = 1000000;  // 1 s
 
 // size class, 32 bytes, the field order of halloc src/size-info.h:8-26
@@ -78,14 +79,17 @@ struct Config {
   uint32_t nib_words_sh;  // log2(words of nibbles per slab) = sb_sh - 7
   uint32_t set_words;     // ceil(nsbs / 32)
   uint32_t sum_words;     // ceil(set_words / 32)
+  uint32_t nheads;        // head slabs per size, a power of two <= kMaxHeads
 };
 
 // mutable allocator state (global memory, one instance per device)
+// per-head arrays are indexed [ihead * kNSizes + size]; head 0 is the one
+// the reference has
 struct State {
-  uint32_t ticket[kNSizes * kTicketStride];
-  uint32_t head_lock[kNSizes * kTicketStride];
-  alignas(128) uint32_t head[kNSizes];
-  uint32_t cached[kNSizes];
+  uint32_t ticket[kMaxHeads * kNSizes * kTicketStride];
+  uint32_t head_lock[kMaxHeads * kNSizes * kTicketStride];
+  alignas(128) uint32_t head[kMaxHeads * kNSizes];
+  uint32_t cached[kMaxHeads * kNSizes];
   alignas(128) uint32_t status;
   uint32_t wait_limit_us;
   uint32_t n_head_changes;

@@ -78,6 +78,8 @@ constexpr int kMaxDevices = 64;
 HostDev g_dev[kMaxDevices];
 // hash-step scale for the next init, in percent (100 = the reference rule)
 uint32_t g_hash_scale_pct = 100;
+// head slabs per size for the next init (1 = the reference policy)
+uint32_t g_nheads = 1;
 
 #define HA_CK(call)                                   \
   do {                                                \
@@ -228,7 +230,7 @@ int init_impl(const ha_opts_c &o) {
   if (!st) rc = HA_ECUDA;
   if (rc == HA_OK) {
     memset(st, 0, sizeof(*st));
-    for (uint32_t s = 0; s < ha::kNSizes; s++) {
+    for (uint32_t s = 0; s < ha::kMaxHeads * ha::kNSizes; s++) {
       st->ticket[s * ha::kTicketStride] = ha::kFirstTicket;
       st->head[s] = ha::kNone;
       st->cached[s] = ha::kNone;
@@ -253,6 +255,7 @@ int init_impl(const ha_opts_c &o) {
     cfg.nib_words_sh = sb_sh - 7;
     cfg.set_words = (uint32_t)((nsbs + 31) / 32);
     cfg.sum_words = (cfg.set_words + 31) / 32;
+    cfg.nheads = g_nheads;
     if (cudaMemset(meta, 0, meta_bytes) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_cls, cls, sizeof(cls)) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_mod, mod, sizeof(mod)) != cudaSuccess ||
@@ -512,6 +515,12 @@ extern "C" int ha_dump_state_c(const ha_state_dump_t *d) {
   if (d->bits) HA_CK(cudaMemcpy(d->bits, h->meta, bit_words * 4, cudaMemcpyDeviceToHost));
   if (d->nibbles)
     HA_CK(cudaMemcpy(d->nibbles, h->meta + bit_words, nib_words * 4, cudaMemcpyDeviceToHost));
+  return HA_OK;
+}
+
+extern "C" int ha_set_heads_c(uint32_t nheads) {
+  if (nheads == 0 || nheads > ha::kMaxHeads || (nheads & (nheads - 1))) return HA_EINVAL;
+  g_nheads = nheads;
   return HA_OK;
 }
 

@@ -114,6 +114,15 @@ int ha_l2_persist_c(void *stream);
    whose addresses match it; the autotuner may pick another. 10..1000. */
 int ha_set_hash_scale_c(uint32_t percent);
 
+/* Tuning knob, applied by the next init on this process: head slabs per
+   size class, a power of two up to 8.  A warp allocates from head
+   (SM id mod nheads), each head with its own ticket counter and its own
+   head replacement, which spreads the hottest words and the replacement
+   work over several slabs.  1 (the default) is the reference policy (its
+   compile-time NHEADS, halloc src/slab.h:43) and the only setting whose
+   addresses match it. */
+int ha_set_heads_c(uint32_t nheads);
+
 /* Test hook for failure detection: sets the head-replacement lock of size
    class `size_id` to `held` (1 = held by a holder that never releases it,
    0 = free).  A hamalloc that then needs a new head for that size waits

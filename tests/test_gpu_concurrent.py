@@ -201,3 +201,34 @@ def test_stats_and_extfrag(torch_cuda):
         assert st["pool_base"] % (4 << 20) == 0
         f = H.extfrag(False)
         assert 0.0 <= f <= 1.0
+
+
+@pytest.mark.parametrize("nheads", [2, 8])
+def test_multi_head_variant(torch_cuda, nheads):
+    """The tuned variant with several head slabs per size keeps every
+    invariant and the exact slab state.  Each (head, size) pair holds a head
+    and a prefetched slab, so the pool is sized for 2 x nheads x 12 sizes
+    slabs beside the data."""
+    import halloc_b200
+    torch = torch_cuda
+    n, k = 131072, 4
+    rng = np.random.default_rng(nheads)
+    sizes = rng.choice(SMALL + [384, 1024, 3072], n * k)
+    halloc_b200.set_heads(nheads)
+    try:
+        with allocator(memory=4 << 30) as H:
+            st = H.stats()
+            ptrs = malloc_batch(torch, H, sizes, n, k)
+            p = ptrs.cpu().numpy()
+            check_blocks(p, sizes, st["pool_base"], st["pool_bytes"])
+            assert_state_matches_live(H, p, sizes)
+            H.free_batch(ptrs, n, k)
+            torch.cuda.synchronize()
+            assert_empty(H)
+            out = torch.zeros(2, dtype=torch.int64, device="cuda")
+            H.throughput(out, 32768, nbytes=16, block=128, nallocs=2, niters=5)
+            torch.cuda.synchronize()
+            assert out.cpu().tolist() == [plain_checksum(32768, 10), 0]
+            assert H.status() == 0
+    finally:
+        halloc_b200.set_heads(1)
