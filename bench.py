@@ -36,7 +36,7 @@ PAIRS_PER_STEP = NTHREADS * NITERS * NALLOCS
 ATOMICS_PER_PAIR = 2  # one bit-array reservation + one release
 # DRAM bytes (read + write) of one launch of the plain kernel, from an ncu
 # capture of the current build (the bench cannot read DRAM counters itself)
-PLAIN_DRAM_BYTES_PER_LAUNCH = 412672
+PLAIN_DRAM_BYTES_PER_LAUNCH = 186368
 METRIC = "16B malloc/free pairs/s"
 WORKLOAD = ("plain: 256 blocks x 128 threads, hamalloc(16) + 16-B write + read-back + hafree, "
             "10 iterations per thread, 512 MiB pool, default halloc_opts_t")
@@ -45,6 +45,22 @@ WORKLOAD = ("plain: 256 blocks x 128 threads, hamalloc(16) + 16-B write + read-b
 def plain_checksum(nthreads: int, per_thread: int) -> int:
     t = np.arange(nthreads, dtype=np.int64)
     return int(per_thread * (4 * (t - t % 4) + 6).sum())
+
+
+def reduce_max_over_ranks(torch, values, world: int, device: str) -> list:
+    """Element-wise max of per-rank values (the timing rule: the slowest
+    replica sets the time); a plain list when there is one rank."""
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def replica_throughput(units_per_rank: float, world: int, max_seconds: float) -> float:
+    """Whole-job throughput of independent replicas: every rank processed
+    units_per_rank units; the job took as long as its slowest rank."""
+    return units_per_rank * world / max_seconds
 
 
 def dist_env():
@@ -230,11 +246,8 @@ def run_ours(args, rank, world, local_rank):
                    int(h_out[0]) == plain_checksum(NTHREADS, NITERS * NALLOCS))
 
     # max over ranks
-    t = torch.tensor([total_s, e2e_s, 0.0 if ok and e2e_ok else 1.0], dtype=torch.float64,
-                     device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_s, e2e_s, bad = t.tolist()
+    total_s, e2e_s, bad = reduce_max_over_ranks(
+        torch, [total_s, e2e_s, 0.0 if ok and e2e_ok else 1.0], world, "cuda")
 
     res = {"step_ms": step_ms, "total_s": total_s, "e2e_s": e2e_s, "ok": bad == 0.0,
            "clocks": clock_summary}
@@ -272,6 +285,28 @@ def run_ours(args, rank, world, local_rank):
     return res
 
 
+def run_atomic_probe(torch, H) -> dict:
+    """32-bit atom.or throughput against the number of distinct words all
+    threads hit (1 word = every thread on one address)."""
+    nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    nthreads = nsm * 2048
+    buf = torch.zeros(nthreads, dtype=torch.int32, device="cuda")
+    out = {}
+    for nwords in (1, 2, 18, 64, 1024, nthreads):
+        reps = 64 if nwords < 100 else 256
+        for ret in (True, False):
+            H.atomic_peak(buf, nwords, nthreads, reps, ret)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            H.atomic_peak(buf, nwords, nthreads, reps, ret)
+            e1.record()
+            e1.synchronize()
+            key = f"words={nwords} {'returning' if ret else 'fire_and_forget'}"
+            out[key] = nthreads * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
+    return {"unit": "G ops/s", "threads": nthreads, "results": out}
+
+
 def run_leg(name: str) -> dict:
     """A secondary workload in a child process: its own CUDA context, so
     its pool and CUDA-heap sizes are set afresh."""
@@ -302,6 +337,8 @@ def leg_main(args):
         out = run_graph(torch, H, 3)
     elif args.leg == "serve":
         out = run_serve(torch, H)
+    elif args.leg == "atomics":
+        out = run_atomic_probe(torch, H)
     else:
         out = run_batched(torch, H, 3, not args.no_tune)
     print("LEG " + json.dumps(out), flush=True)
@@ -560,8 +597,8 @@ def main_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     res = run_ours(args, rank, world, local_rank)
     if rank == 0:
-        value = PAIRS_PER_STEP * args.steps * world / res["total_s"]
-        e2e = PAIRS_PER_STEP * args.steps * world / res["e2e_s"]
+        value = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["total_s"])
+        e2e = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["e2e_s"])
         if args.only_gpu:
             print(json.dumps({"metric": METRIC, "value": value, "e2e": e2e, "ok": res["ok"],
                               "note": "GPU legs only (profiling run)"}), flush=True)
@@ -660,7 +697,7 @@ def main():
     p.add_argument("--no-tune", action="store_true", help="batched leg without the autotuner")
     p.add_argument("--skip-graph", action="store_true", help="skip the random-graph leg")
     p.add_argument("--skip-serve", action="store_true", help="skip the serving leg")
-    p.add_argument("--leg", choices=["phase", "batched", "graph", "serve"],
+    p.add_argument("--leg", choices=["phase", "batched", "graph", "serve", "atomics"],
                    help=argparse.SUPPRESS)
     p.add_argument("--only-gpu", action="store_true",
                    help="skip the CPU and CUDA-malloc legs (profiling runs)")

@@ -72,4 +72,14 @@ void ha_shutdown(void);
     allocatable.  (replaces halloc src/halloc.h:55) */
 double ha_extfrag(bool ideal);
 
+/* Device operator new / delete served by hamalloc / hafree, when the
+   program is compiled with -DHALLOC_CPP and linked with libhalloc_cpp.a
+   (replaces halloc src/halloc.h:71-80, disabled there).  Only the scalar
+   forms are replaced, as in the original. */
+#if defined(HALLOC_CPP)
+__device__ void *operator new(size_t nbytes);
+__device__ void operator delete(void *p) noexcept;
+__device__ void operator delete(void *p, size_t nbytes) noexcept;
+#endif
+
 #endif

@@ -7,22 +7,42 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-SRC = os.path.join(ROOT, "tests", "dropin", "user_kernel.cu")
-BIN = os.path.join(ROOT, "tests", "dropin", "_build", "user_kernel")
+DROPIN = os.path.join(ROOT, "tests", "dropin")
+
+
+def _build(name: str, lib: str, defines: list, force: bool) -> str:
+    from halloc_b200.build import ARCH, INCLUDE, nvcc
+    src = os.path.join(DROPIN, name + ".cu")
+    exe = os.path.join(DROPIN, "_build", name)
+    if not force and os.path.exists(exe) and os.path.getmtime(exe) >= max(
+            os.path.getmtime(src), os.path.getmtime(lib)):
+        return exe
+    os.makedirs(os.path.dirname(exe), exist_ok=True)
+    obj = exe + ".o"
+    subprocess.run([nvcc()] + ARCH + ["-O3", "-rdc=true", "-I" + INCLUDE] + defines +
+                   ["-c", src, "-o", obj], check=True)
+    subprocess.run([nvcc()] + ARCH + [obj, lib, "-o", exe], check=True)
+    return exe
 
 
 def build_dropin_sample(force: bool = False) -> str:
     """nvcc -rdc=true user_kernel.cu + libhalloc.a -> tests/dropin/_build."""
-    from halloc_b200.build import ARCH, INCLUDE, LIB_A, nvcc
-    if not force and os.path.exists(BIN) and os.path.getmtime(BIN) >= max(
-            os.path.getmtime(SRC), os.path.getmtime(LIB_A)):
-        return BIN
-    os.makedirs(os.path.dirname(BIN), exist_ok=True)
-    obj = BIN + ".o"
-    subprocess.run([nvcc()] + ARCH + ["-O3", "-rdc=true", "-I" + INCLUDE, "-c", SRC, "-o", obj],
-                   check=True)
-    subprocess.run([nvcc()] + ARCH + [obj, LIB_A, "-o", BIN], check=True)
-    return BIN
+    from halloc_b200.build import LIB_A
+    return _build("user_kernel", LIB_A, [], force)
+
+
+def build_new_delete_sample(force: bool = False) -> str:
+    """user_new.cu with -DHALLOC_CPP + libhalloc_cpp.a -> tests/dropin/_build."""
+    from halloc_b200.build import LIB_CPP_A
+    return _build("user_new", LIB_CPP_A, ["-DHALLOC_CPP"], force)
+
+
+@pytest.mark.gpu
+def test_device_new_delete_served_by_the_allocator(torch_cuda):
+    exe = build_new_delete_sample()
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK"), r.stdout
 
 
 @pytest.mark.gpu
