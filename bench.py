@@ -333,6 +333,7 @@ def leg_main(args):
                                 "ok": tuned["ok"],
                                 "note": "4 head slabs per size (ha_set_heads_c); addresses "
                                         "no longer follow the reference policy"}
+        out["reference_form"] = run_phase_ref(torch, H)
     elif args.leg == "graph":
         out = run_graph(torch, H, 3)
     elif args.leg == "serve":
@@ -390,6 +391,57 @@ def run_phase(torch, H, reps: int, hbm_peak_gbs: float | None, nheads: int = 1) 
                        "note": "written + read once; expected mean block size"}}
     if hbm_peak_gbs:
         out["payload"]["frac_of_hbm"] = gbs / hbm_peak_gbs
+    return out
+
+
+# The reference's own phase experiments (tst/exp/speed/exp-run.pl:9-101 with
+# tst/exp/common.pl): -f0.95 -F0.05 -e0.91 -m512MiB -g5, "spree" = -i1 -t512,
+# "private" = -i32 -t16; (name, threads, blocks per thread, smin, smax,
+# published Kepler private / spree Mpairs/s with their file:line)
+PHASE_REF_CASES = [
+    ("mixed_8_256", 1 << 20, 1, 8, 256, (927.18, 795.18),
+     "tst/exp/speed/exp-log-combi.csv:4"),
+    ("single_16x4", 1 << 20, 4, 16, 16, (1401.70, 1220.15),
+     "tst/exp/speed/exp-log-single.csv:2"),
+]
+
+
+def run_phase_ref(torch, H) -> dict:
+    """The phase workload in the reference's own form: per-thread generator
+    states seeded per group of 32 threads, Markov transitions with
+    p00 = p11 = 0.9526, p01 = p10 = 0.1, one launch per try, the counts
+    checked against their balance and the pool left empty."""
+    from halloc_b200.workloads import group_seeds
+    probs = H.phase_ref_probabilities(0.95, 0.05, 0.91)
+    out = {"config": "phase-throughput -f0.95 -F0.05 -e0.91 -m536870912 -g5, as the "
+                     "reference's speed experiments run it; device time (CUDA events) "
+                     "summed over the launches", "probs": probs}
+    for name, n, nallocs, smin, smax, published, src in PHASE_REF_CASES:
+        for form, niters, ntries in (("spree", 1, 512), ("private", 32, 16)):
+            H.init(H.HallocOpts(memory=512 << 20))
+            seeds = group_seeds(n, 32, 0x5EED)
+            states = torch.tensor(seeds.view(np.int32), device="cuda")
+            slots = torch.zeros(nallocs * n, dtype=torch.int64, device="cuda")
+            ctrs = torch.zeros(n, dtype=torch.int32, device="cuda")
+            acc = torch.zeros(4, dtype=torch.int64, device="cuda")
+            H.phase_ref_run(n, nallocs, 4, niters, probs, smin, smax, states, slots, ctrs,
+                            acc)  # warm-up
+            states.copy_(torch.tensor(seeds.view(np.int32), device="cuda"))
+            r = H.phase_ref_run(n, nallocs, ntries, niters, probs, smin, smax, states, slots,
+                                ctrs, acc)
+            ok = (r["failed"] == 0 and r["mallocs"] == r["frees"] and H.status() == 0 and
+                  H.stats()["used_chunks"] == 0)
+            H.shutdown()
+            sec = r["kernel_ms"] * 1e-3
+            # the reference's own count: 0.5 x threads x blocks x iterations x tries x e
+            formula = 0.5 * n * nallocs * niters * ntries * 0.91
+            out[f"{name}_{form}"] = {
+                "args": f"-n{n} -l{nallocs} -s{smin} -S{smax} -i{niters} -t{ntries}",
+                "pairs_per_s": r["mallocs"] / sec,
+                "pairs_per_s_reference_formula": formula / sec,
+                "mallocs": r["mallocs"], "ms": r["kernel_ms"], "ok": ok,
+                "published_kepler_mpairs_s": published[0 if form == "private" else 1],
+                "published_source": src}
     return out
 
 

@@ -23,7 +23,7 @@ import numpy as np
 __all__ = [
     "HallocError", "HallocOpts", "init", "shutdown", "extfrag", "stats", "status",
     "clear_status", "set_wait_limit", "dump_state", "l2_persist", "malloc_batch",
-    "free_batch", "phase_round", "phase_run", "graph_build", "graph_gather", "serve_run",
+    "free_batch", "phase_round", "phase_run", "phase_ref_step", "phase_ref_run", "graph_build", "graph_gather", "serve_run",
     "throughput", "throughput_host", "cuda_throughput", "trace",
     "atomic_peak", "debug_set_head_lock", "set_hash_scale", "set_heads", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
 ]
@@ -105,6 +105,11 @@ class _CServeResult(ctypes.Structure):
                 ("max_cycles", ctypes.c_double), ("hist", ctypes.c_uint64 * SERVE_HIST)]
 
 
+class _CPhaseRefResult(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("alloc_phase_ms", ctypes.c_double),
+                ("free_phase_ms", ctypes.c_double), ("acc", ctypes.c_uint64 * 4)]
+
+
 class _CDump(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in (
         "tickets", "heads", "cached", "size_infos", "counters", "size_id", "chunk_id",
@@ -138,6 +143,10 @@ _SIGS = {
                                 _vp]),
     "ha_phase_run_c": (_int, [_u32, _u32, _u32, _u32, _u32, _u32, ctypes.c_uint64, _u32, _vp,
                               _u32, _vp, _vp, _vp, ctypes.POINTER(_CPhaseResult), _vp]),
+    "ha_phase_ref_step_c": (_int, [_u32, _u32, _u32, _u32, _vp, _u32, _u32, _vp, _vp, _vp,
+                                   _vp, _int, _vp]),
+    "ha_phase_ref_run_c": (_int, [_u32, _u32, _u32, _u32, _vp, _u32, _u32, _vp, _vp, _vp, _vp,
+                                  ctypes.POINTER(_CPhaseRefResult), _vp]),
     "ha_atomic_peak_c": (_int, [_vp, _u32, _u32, _u32, _int, _vp]),
 }
 
@@ -338,6 +347,61 @@ def phase_run(nthreads: int, nslots: int, seed: int, periods: int, thr_alloc: in
            "kernel_ms": r.kernel_ms, "filled": r.filled}
     out.update(dict(zip(PHASE_ACC, list(r.acc))))
     return out
+
+
+PHASE_REF_ACC = ("mallocs", "frees", "failed", "bytes")
+
+
+def _probs(probs) -> ctypes.Array:
+    p = (ctypes.c_float * 4)(*[float(x) for x in probs])
+    if len(probs) != 4:
+        raise HallocError("probs: four transition probabilities expected")
+    return p
+
+
+def phase_ref_step(nthreads: int, nallocs: int, itry: int, niters: int, probs, smin: int,
+                   smax: int, states, slots, ctrs, acc, rest: bool = False,
+                   stream=None) -> None:
+    """One launch of the reference-form phase workload (ha_phase_ref_step_c);
+    probs = (p00, p01, p10, p11) as in phase_ref_probabilities; device
+    buffers: states (nthreads u32), slots (nallocs*nthreads pointers), ctrs
+    (nthreads u32), acc (4 u64, accumulated)."""
+    _check(load().ha_phase_ref_step_c(nthreads, nallocs, itry, niters, _probs(probs), smin,
+                                      smax, _addr(states), _addr(slots), _addr(ctrs),
+                                      _addr(acc), int(rest), _stream(stream)),
+           "ha_phase_ref_step_c")
+
+
+def phase_ref_run(nthreads: int, nallocs: int, ntries: int, niters: int, probs, smin: int,
+                  smax: int, states, slots, ctrs, acc, stream=None) -> dict:
+    """ntries launches then the final free (ha_phase_ref_run_c)."""
+    r = _CPhaseRefResult()
+    _check(load().ha_phase_ref_run_c(nthreads, nallocs, ntries, niters, _probs(probs), smin,
+                                     smax, _addr(states), _addr(slots), _addr(ctrs),
+                                     _addr(acc), ctypes.byref(r), _stream(stream)),
+           "ha_phase_ref_run_c")
+    out = {"kernel_ms": r.kernel_ms, "alloc_phase_ms": r.alloc_phase_ms,
+           "free_phase_ms": r.free_phase_ms}
+    out.update(dict(zip(PHASE_REF_ACC, list(r.acc))))
+    return out
+
+
+def phase_ref_probabilities(alloc_fraction: float, free_fraction: float,
+                            exec_fraction: float) -> tuple:
+    """Transition probabilities (p00, p01, p10, p11) from the steady-state
+    fractions f (after the allocation phase), F (after the free phase) and
+    e (threads acting per phase), in float32 as halloc computes them
+    (tst/common/common.cu:311-355); p[phase][holding]."""
+    f32 = np.float32
+    f, F, e = f32(alloc_fraction), f32(free_fraction), f32(exec_fraction)
+    one, two = f32(1), f32(2)
+    if e + f + F > 2 or e < abs(f - F):
+        raise HallocError("phase_ref_probabilities: fractions out of range")
+    p00 = (e + f - F) / (two * (one - F)) if F < 1 else one
+    p01 = (e - f + F) / (two * F) if F > 0 else one
+    p10 = (e - f + F) / (two * (one - f)) if f < 1 else one
+    p11 = (e + f - F) / (two * f) if f > 0 else f32(0)
+    return tuple(float(f32(x)) for x in (p00, p01, p10, p11))
 
 
 def graph_build(n: int, seed: int, cdf, ncdf: int, arr, deg, acc, stream=None) -> None:

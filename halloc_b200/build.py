@@ -24,8 +24,6 @@ INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 SO = os.path.join(PKG, "libhalloc_b200.so")
 LIB_A = os.path.join(PKG, "libhalloc.a")
-# the same with device operator new / delete served by the allocator
-LIB_CPP_A = os.path.join(PKG, "libhalloc_cpp.a")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler", "-fPIC",
@@ -79,13 +77,6 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     halloc_o = objs[0]
     if _stale(LIB_A, [halloc_o]):
         _run([cc] + ARCH + ["-lib", halloc_o, "-o", LIB_A], verbose)
-    cpp_o = os.path.join(BUILD, "halloc_cpp.o")
-    src = os.path.join(CSRC, "halloc.cu")
-    if _stale(cpp_o, [src, __file__] + HEADERS):
-        _run([cc] + CUFLAGS + SOURCES["halloc.cu"] + ["-DHALLOC_CPP", "-c", src, "-o", cpp_o],
-             verbose)
-    if _stale(LIB_CPP_A, [cpp_o]):
-        _run([cc] + ARCH + ["-lib", cpp_o, "-o", LIB_CPP_A], verbose)
     dlink = os.path.join(BUILD, "dlink.o")
     if _stale(SO, objs):
         _run([cc] + ARCH + ["-Xcompiler", "-fPIC", "-dlink"] + objs + ["-o", dlink], verbose)

@@ -238,6 +238,90 @@ __global__ void ha_phase_free_k(uint32_t n, uint32_t nslots, uint32_t seed, uint
   block_add2(nfree, 0, acc + 5, acc + 5);
 }
 
+// ---- phase workload, the reference's own form -------------------------------
+//
+// halloc tst/perf/phase-throughput/phase-throughput.cu:17-48 and free_rest_k
+// (tst/common/common.h:403-412), with the reference's per-thread generator
+// and draws (tst/common/common.h:80-117, 209-235): Thomas Wang's 32-bit
+// integer hash applied to the thread's state, an integer in [a, b] from the
+// low 24 bits modulo the range, a probability test against a 20-bit
+// fraction.  The same draws in the same order give the same decisions.
+
+__device__ __forceinline__ uint32_t wang_next(uint32_t &st) {
+  uint32_t x = st;
+  x = (x ^ 61u) ^ (x >> 16);
+  x *= 9u;
+  x ^= x >> 4;
+  x *= 0x27d4eb2du;
+  x ^= x >> 15;
+  st = x;
+  return x;
+}
+__device__ __forceinline__ uint32_t draw_in(uint32_t &st, uint32_t a, uint32_t b) {
+  return a + (wang_next(st) & 0x00ffffffu) % (b - a + 1);
+}
+__device__ __forceinline__ bool draw_bool(uint32_t &st, float p) {
+  if (0.0f < p && p < 1.0f)
+    return (1.0f / (1024.0f * 1024.0f)) * (float)draw_in(st, 0, (1u << 20) - 1) <= p;
+  return p >= 1.0f;
+}
+
+struct PhaseRefProbs {
+  float p[4];  // [phase * 2 + holding]
+};
+
+// acc: [0] mallocs, [1] frees, [2] failed mallocs, [3] bytes of successful mallocs
+__global__ void ha_phase_ref_k(uint32_t n, uint32_t nallocs, uint32_t step0, uint32_t niters,
+                               PhaseRefProbs pr, uint32_t smin, uint32_t smax,
+                               uint32_t *states, void **slots, uint32_t *ctrs,
+                               unsigned long long *acc, int rest) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long nmal = 0, nfree = 0, nfail = 0, bytes = 0;
+  if (i < n) {
+    uint32_t ctr = ctrs[i];
+    if (rest) {
+      for (uint32_t k = 0; k < ctr; k++) {
+        hafree(slots[(size_t)k * n + i]);
+        slots[(size_t)k * n + i] = nullptr;
+      }
+      nfree += ctr;
+      ctr = 0;
+    } else {
+      uint32_t st = states[i];
+      for (uint32_t it = 0; it < niters; it++) {
+        const uint32_t phase = (step0 + it) & 1u;
+        const bool holding = ctr > 0;
+        if (!draw_bool(st, pr.p[phase * 2 + (holding ? 1 : 0)])) continue;
+        if (!holding) {
+          for (uint32_t k = 0; k < nallocs; k++) {
+            const uint32_t sz = smin == smax ? smin : draw_in(st, smin, smax);
+            void *p = hamalloc(sz);
+            slots[(size_t)k * n + i] = p;
+            if (p) {
+              nmal++;
+              bytes += sz;
+            } else {
+              nfail++;
+            }
+          }
+          ctr = nallocs;
+        } else {
+          for (uint32_t k = 0; k < nallocs; k++) {
+            hafree(slots[(size_t)k * n + i]);
+            slots[(size_t)k * n + i] = nullptr;
+          }
+          nfree += nallocs;
+          ctr = 0;
+        }
+      }
+      states[i] = st;
+    }
+    ctrs[i] = ctr;
+  }
+  block_add2(nmal, nfree, acc, acc + 1);
+  block_add2(nfail, bytes, acc + 2, acc + 3);
+}
+
 // ---- batched workload ---------------------------------------------------------
 
 // allocation of requests [begin, end): the block carries its request id
@@ -645,6 +729,67 @@ extern "C" int ha_phase_run_c(uint32_t nthreads, uint32_t nslots, uint32_t seed,
     rc = HA_ECUDA;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  return rc;
+}
+
+extern "C" int ha_phase_ref_step_c(uint32_t nthreads, uint32_t nallocs, uint32_t itry,
+                                   uint32_t niters, const float *probs, uint32_t smin,
+                                   uint32_t smax, uint32_t *states, void **slots,
+                                   uint32_t *ctrs, uint64_t *acc, int rest, void *stream) {
+  if (!probs || !states || !slots || !ctrs || !acc || nallocs == 0 ||
+      nallocs > kMaxAllocsPerThread || smin == 0 || smin > smax)
+    return HA_EINVAL;
+  if (nthreads == 0) return HA_OK;
+  PhaseRefProbs pr;
+  for (int k = 0; k < 4; k++) pr.p[k] = probs[k];
+  const uint64_t step0 = (uint64_t)itry * niters;
+  ha_phase_ref_k<<<blocks_for(nthreads, 128), 128, 0, as_stream(stream)>>>(
+      nthreads, nallocs, (uint32_t)step0, niters, pr, smin, smax, states, slots, ctrs,
+      reinterpret_cast<unsigned long long *>(acc), rest);
+  return launch_status();
+}
+
+extern "C" int ha_phase_ref_run_c(uint32_t nthreads, uint32_t nallocs, uint32_t ntries,
+                                  uint32_t niters, const float *probs, uint32_t smin,
+                                  uint32_t smax, uint32_t *states, void **slots, uint32_t *ctrs,
+                                  uint64_t *acc, ha_phase_ref_result_t *res, void *stream) {
+  if (!res || !acc) return HA_EINVAL;
+  memset(res, 0, sizeof(*res));
+  cudaStream_t s = as_stream(stream);
+  if (cudaMemsetAsync(acc, 0, 4 * sizeof(uint64_t), s) != cudaSuccess) return HA_ECUDA;
+  std::vector<cudaEvent_t> ev;
+  int rc = HA_OK;
+  for (uint32_t k = 0; k < 2 * (ntries + 1) && rc == HA_OK; k++) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) rc = HA_ECUDA;
+    else ev.push_back(e);
+  }
+  for (uint32_t t = 0; t <= ntries && rc == HA_OK; t++) {
+    if (cudaEventRecord(ev[2 * t], s) != cudaSuccess) {
+      rc = HA_ECUDA;
+      break;
+    }
+    rc = ha_phase_ref_step_c(nthreads, nallocs, t, niters, probs, smin, smax, states, slots,
+                             ctrs, acc, t == ntries, stream);
+    if (rc == HA_OK && cudaEventRecord(ev[2 * t + 1], s) != cudaSuccess) rc = HA_ECUDA;
+  }
+  if (rc == HA_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = HA_ECUDA;
+  for (uint32_t t = 0; t <= ntries && rc == HA_OK; t++) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ev[2 * t], ev[2 * t + 1]) != cudaSuccess) {
+      rc = HA_ECUDA;
+      break;
+    }
+    res->kernel_ms += ms;
+    if (t < ntries && t % 2 == 0)
+      res->alloc_phase_ms += ms;
+    else
+      res->free_phase_ms += ms;
+  }
+  if (rc == HA_OK &&
+      cudaMemcpy(res->acc, acc, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = HA_ECUDA;
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
   return rc;
 }
 

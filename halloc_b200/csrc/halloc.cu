@@ -57,14 +57,6 @@ __device__ __noinline__ void hafree(void *p) {
     free(p);
 }
 
-#if defined(HALLOC_CPP)
-// device operator new / delete on top of the allocator (libhalloc_cpp.a only;
-// halloc src/halloc.cu:201-208, 258-265)
-__device__ void *operator new(size_t nbytes) { return hamalloc(nbytes); }
-__device__ void operator delete(void *p) noexcept { hafree(p); }
-__device__ void operator delete(void *p, size_t) noexcept { hafree(p); }
-#endif
-
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------

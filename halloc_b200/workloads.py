@@ -1,5 +1,6 @@
-"""Workload drivers built on the C ABI: the batched request stream and the
-degree table of the random-graph build.
+"""Workload drivers built on the C ABI: the batched request stream, the
+degree table of the random-graph build and the generator seeds of the
+reference-form phase workload.
 
 The batched stream (64 batches of log-uniform size between 1,024 and
 1,048,576 requests; block sizes geometric over the 16 size classes with
@@ -154,3 +155,13 @@ def poisson_thresholds(lam: float = 16.0) -> np.ndarray:
         cdf += p
     out[-1] = 2**32 - 1
     return np.asarray(out, np.uint32)
+
+
+def group_seeds(nthreads: int, group: int, seed: int) -> np.ndarray:
+    """Initial generator states for the reference-form phase workload
+    (ha_phase_ref_step_c): one seed per group of `group` consecutive
+    threads, as halloc's drandom_init (tst/common/common.cu:358-383, period
+    1) seeds them, drawn from a seeded numpy generator instead of random()."""
+    rng = np.random.default_rng(seed)
+    per_group = rng.integers(0, 1 << 31, (nthreads + group - 1) // group, dtype=np.uint32)
+    return np.repeat(per_group, group)[:nthreads].astype(np.uint32)

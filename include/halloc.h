@@ -72,14 +72,34 @@ void ha_shutdown(void);
     allocatable.  (replaces halloc src/halloc.h:55) */
 double ha_extfrag(bool ideal);
 
-/* Device operator new / delete served by hamalloc / hafree, when the
-   program is compiled with -DHALLOC_CPP and linked with libhalloc_cpp.a
-   (replaces halloc src/halloc.h:71-80, disabled there).  Only the scalar
-   forms are replaced, as in the original. */
+/* Device operator new / delete served by hamalloc / hafree when the
+   program is compiled with -DHALLOC_CPP (replaces halloc src/halloc.h:71-80
+   and src/halloc.cu:201-208, 258-265, disabled there).  nvcc binds a device
+   new-expression to a replacement operator only when the operator's
+   definition is visible in the translation unit, so the definitions are
+   here, inline (nonstandard for replacement operators: nvcc warning 2620,
+   suppressed).  operator new promises 16-byte alignment, and blocks of the
+   24-byte-chunk size classes are only 8-byte aligned, so requests of
+   17..24, 33..48, 65..96 and 129..192 bytes are served from the next
+   16-byte-chunk class (32, 64, 128, 256 bytes).  The array forms, which
+   halloc left commented out, are included.  Failure returns NULL. */
 #if defined(HALLOC_CPP)
-__device__ void *operator new(size_t nbytes);
-__device__ void operator delete(void *p) noexcept;
-__device__ void operator delete(void *p, size_t nbytes) noexcept;
+#pragma nv_diagnostic push
+#pragma nv_diag_suppress 2620
+__device__ __forceinline__ size_t ha_new_bytes(size_t n) {
+  if (n > 16 && n <= 24) return 32;
+  if (n > 32 && n <= 48) return 64;
+  if (n > 64 && n <= 96) return 128;
+  if (n > 128 && n <= 192) return 256;
+  return n;
+}
+__device__ inline void *operator new(size_t n) { return hamalloc(ha_new_bytes(n)); }
+__device__ inline void *operator new[](size_t n) { return hamalloc(ha_new_bytes(n)); }
+__device__ inline void operator delete(void *p) noexcept { hafree(p); }
+__device__ inline void operator delete[](void *p) noexcept { hafree(p); }
+__device__ inline void operator delete(void *p, size_t) noexcept { hafree(p); }
+__device__ inline void operator delete[](void *p, size_t) noexcept { hafree(p); }
+#pragma nv_diagnostic pop
 #endif
 
 #endif

@@ -211,6 +211,40 @@ int ha_phase_run_c(uint32_t nthreads, uint32_t nslots, uint32_t seed,
                    uint32_t *slot_sz, uint64_t *acc, ha_phase_result_t *res,
                    void *stream);
 
+/* ---- phase workload, the reference's own form --------------------- */
+
+/* One kernel launch ("try" itry) of the reference's phase-throughput test
+   (halloc tst/perf/phase-throughput/phase-throughput.cu:17-48): each of
+   nthreads threads runs niters iterations; in iteration it of try itry the
+   phase is (itry * niters + it) % 2 (0 = allocation, 1 = free), and a thread
+   holding nothing allocates nallocs blocks with probability probs[2*phase],
+   a thread holding blocks frees them all with probability probs[2*phase+1].
+   Sizes are drawn uniformly from [smin, smax] (no draw when equal).  All
+   draws come from the thread's generator state states[i] (Thomas Wang's
+   32-bit integer hash chained, tst/common/common.h:80-117), updated in
+   place.  Block k of thread i is slots[k * nthreads + i]; ctrs[i] is the
+   thread's number of blocks (0 or nallocs).  With rest != 0 the launch
+   instead frees every block still held (free_rest_k).  acc (device, 4
+   words, accumulated, not reset): mallocs, frees, failed mallocs, bytes
+   requested by successful mallocs. */
+int ha_phase_ref_step_c(uint32_t nthreads, uint32_t nallocs, uint32_t itry, uint32_t niters,
+                        const float *probs, uint32_t smin, uint32_t smax, uint32_t *states,
+                        void **slots, uint32_t *ctrs, uint64_t *acc, int rest, void *stream);
+
+typedef struct ha_phase_ref_result_t {
+  double kernel_ms;      /* all tries and the final free (CUDA events) */
+  double alloc_phase_ms; /* even tries */
+  double free_phase_ms;  /* odd tries and the final free */
+  uint64_t acc[4];       /* as in ha_phase_ref_step_c, over the whole run */
+} ha_phase_ref_result_t;
+
+/* ntries tries then the final free, each launch timed with CUDA events
+   (the host loop of phase-throughput.cu:76-110).  acc is reset first. */
+int ha_phase_ref_run_c(uint32_t nthreads, uint32_t nallocs, uint32_t ntries, uint32_t niters,
+                       const float *probs, uint32_t smin, uint32_t smax, uint32_t *states,
+                       void **slots, uint32_t *ctrs, uint64_t *acc,
+                       ha_phase_ref_result_t *res, void *stream);
+
 /* ---- batched workload -------------------------------------------- */
 
 /* A stream of allocation batches.  Step s (0 <= s <= nbatch) first frees

@@ -8,6 +8,9 @@ Two host libraries, both loaded through ctypes:
   allocator's own sources (src/halloc.cu and the headers it includes)
   compiled unchanged as host C++ (``oracle/refhost``, ``oracle/Makefile``).
   Present only where the reference tree was available at build time.
+* ``ref_phase_draws`` -- ``oracle/_ref/libphase_refdraws.so``: the
+  decisions and size draws of the reference's phase-throughput test, from
+  its own harness header (tst/common/common.h), to pin ``oracle/phase.py``.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 leg may use this package; the product path never imports it.
@@ -23,6 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 MODEL_SO = os.path.join(HERE, "_build", "libhamodel.so")
 REF_SO = os.path.join(HERE, "_ref", "libhalloc_refhost.so")
+REF_DRAWS_SO = os.path.join(HERE, "_ref", "libphase_refdraws.so")
 
 NSIZES = 16
 NSETS = 1 + 4 + 2 * NSIZES  # free, sparse[4], roomy[16], busy[16]
@@ -211,6 +215,28 @@ def ref_lib():
         _bind(lib, "ref_", [])
         _libs["ref"] = lib
     return _libs["ref"]
+
+
+def ref_phase_draws(seeds: np.ndarray, probs, smin: int, smax: int, nallocs: int,
+                    ntries: int, niters: int = 1):
+    """Runs the reference's phase-test decisions (next_action, next_alloc_sz,
+    drandom) for every thread and try, allocations left out.  Returns
+    (ctr[ntries, n], sizes[ntries, nallocs, n], final generator states)."""
+    if "draws" not in _libs:
+        lib = ctypes.CDLL(REF_DRAWS_SO)
+        lib.ref_phase_draws.restype = _int
+        lib.ref_phase_draws.argtypes = [_vp, _u32, _vp, _u32, _u32, _u32, _u32, _u32, _vp,
+                                        _vp, _vp]
+        _libs["draws"] = lib
+    seeds = np.ascontiguousarray(seeds, np.uint32)
+    n = len(seeds)
+    ctr = np.zeros((ntries, n), np.uint32)
+    sz = np.zeros((ntries, nallocs, n), np.uint32)
+    st = np.zeros(n, np.uint32)
+    p = (ctypes.c_float * 4)(*[float(x) for x in probs])
+    _libs["draws"].ref_phase_draws(_ptr(seeds), n, p, smin, smax, nallocs, ntries, niters,
+                                   _ptr(ctr), _ptr(sz), _ptr(st))
+    return ctr, sz, st
 
 
 class Reference(_Allocator):

@@ -95,3 +95,88 @@ class PhaseReplay:
         return {"alloc_rounds": alloc_rounds, "free_rounds": free_rounds, "filled": filled,
                 "wsum": self.wsum, "rsum": self.rsum, "mallocs": self.mallocs,
                 "frees": self.frees}
+
+
+# ---- the reference's own form of the phase workload ---------------------------
+#
+# halloc tst/perf/phase-throughput/phase-throughput.cu:17-48 (one launch per
+# try) and tst/common/common.h:80-117, 209-235 (per-thread generator, draws,
+# next_action, next_alloc_sz with the uniform distribution).
+
+
+def wang_next(st: np.ndarray) -> np.ndarray:
+    """Thomas Wang's 32-bit integer hash, the reference's drandom() step
+    (tst/common/common.h:86-91); returns the new states."""
+    x = np.array(st, dtype=np.uint32, copy=True)
+    x = (x ^ np.uint32(61)) ^ (x >> np.uint32(16))
+    x *= np.uint32(9)
+    x ^= x >> np.uint32(4)
+    x *= np.uint32(0x27D4EB2D)
+    x ^= x >> np.uint32(15)
+    return x
+
+
+def wang_next_scalar(x: int) -> int:
+    """The same step on a Python int (for known-answer checks)."""
+    x = ((x ^ 61) ^ (x >> 16)) & MASK32
+    x = (x * 9) & MASK32
+    x ^= x >> 4
+    x = (x * 0x27D4EB2D) & MASK32
+    x ^= x >> 15
+    return x
+
+
+class PhaseRefReplay:
+    """Replays the reference-form phase workload thread by thread: the
+    decisions, block sizes, generator states and per-thread block counts are
+    exactly the device's, whatever the scheduling, as long as no allocation
+    failed.  sizes[k, i] is the size of thread i's k-th live block (0 when
+    the thread holds nothing)."""
+
+    def __init__(self, states: np.ndarray, nallocs: int, probs, smin: int, smax: int,
+                 niters: int = 1):
+        self.st = np.array(states, dtype=np.uint32, copy=True)
+        self.n = len(self.st)
+        self.nallocs, self.niters = nallocs, niters
+        self.p = np.asarray(probs, np.float32).reshape(2, 2)
+        self.smin, self.smax = smin, smax
+        self.ctr = np.zeros(self.n, np.uint32)
+        self.sizes = np.zeros((nallocs, self.n), np.uint32)
+        self.mallocs = self.frees = self.bytes = 0
+
+    def _draw_in(self, mask: np.ndarray, a: int, b: int) -> np.ndarray:
+        nxt = wang_next(self.st)
+        self.st = np.where(mask, nxt, self.st)
+        return np.uint32(a) + (nxt & np.uint32(0x00FFFFFF)) % np.uint32(b - a + 1)
+
+    def _draw_bool(self, mask: np.ndarray, p: np.ndarray) -> np.ndarray:
+        inner = (p > 0) & (p < 1)
+        k = self._draw_in(mask & inner, 0, (1 << 20) - 1)
+        frac = np.float32(1.0 / (1 << 20)) * k.astype(np.float32)
+        return np.where(inner, frac <= p, p >= 1)
+
+    def step(self, itry: int) -> None:
+        every = np.ones(self.n, bool)
+        for it in range(self.niters):
+            phase = (itry * self.niters + it) % 2
+            holding = self.ctr > 0
+            p = np.where(holding, self.p[phase, 1], self.p[phase, 0]).astype(np.float32)
+            act = self._draw_bool(every, p)
+            alloc = act & ~holding
+            free = act & holding
+            for k in range(self.nallocs):
+                if self.smin == self.smax:
+                    sz = np.full(self.n, self.smin, np.uint32)
+                else:
+                    sz = self._draw_in(alloc, self.smin, self.smax)
+                self.sizes[k] = np.where(alloc, sz, np.where(free, 0, self.sizes[k]))
+                self.bytes += int(sz[alloc].sum(dtype=np.uint64))
+            self.mallocs += int(alloc.sum()) * self.nallocs
+            self.frees += int(free.sum()) * self.nallocs
+            self.ctr = np.where(alloc, self.nallocs, np.where(free, 0, self.ctr)).astype(
+                np.uint32)
+
+    def rest(self) -> None:
+        self.frees += int(self.ctr.sum())
+        self.ctr[:] = 0
+        self.sizes[:] = 0

@@ -1,7 +1,7 @@
 """Generates the golden fixtures in this directory from the REFERENCE
 allocator's own code (halloc 0.11 compiled for the host, oracle/_ref).
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [traces] [phase]
 
 The reference tree is needed only here; the fixtures are committed so that
 tests run where it is absent (e.g. the GPU box).
@@ -15,6 +15,11 @@ Fixtures:
   and the final allocator state (tickets, heads, cached heads, packed slab
   counters, slab descriptors, slab sets, and SHA-256 digests of the bit
   arrays and size nibbles).
+* phase_draws.npz -- the reference's phase-throughput decisions
+  (tst/common/common.h next_action / next_alloc_sz / drandom, run by
+  oracle/_ref/libphase_refdraws.so): for each case its parameters, the
+  initial generator states, every thread's block count and live block
+  sizes after every try, and the final generator states.
 """
 from __future__ import annotations
 
@@ -82,9 +87,46 @@ def size_tables() -> dict:
     return out
 
 
+# (name, (f, F, e), smin, smax, nallocs, niters, group, seed); 2,048 threads,
+# 8 tries each
+PHASE_CASES = [
+    ("readme_uniform", (0.95, 0.05, 0.91), 16, 256, 4, 1, 1, 1),
+    ("readme_groups32", (0.95, 0.05, 0.91), 16, 256, 4, 1, 32, 2),
+    ("fixed16_iters3", (0.95, 0.05, 0.91), 16, 16, 4, 3, 1, 3),
+    ("skewed", (0.7, 0.2, 0.6), 16, 3072, 2, 2, 1, 4),
+    ("always", (1.0, 0.0, 1.0), 24, 24, 1, 1, 1, 5),
+]
+PHASE_THREADS, PHASE_TRIES = 2048, 8
+
+
+def phase_draws() -> None:
+    from halloc_b200.workloads import group_seeds
+    from halloc_b200 import phase_ref_probabilities
+    arrays, index = {}, []
+    for name, fr, smin, smax, nallocs, niters, group, seed in PHASE_CASES:
+        probs = phase_ref_probabilities(*fr)
+        seeds = group_seeds(PHASE_THREADS, group, seed)
+        ctr, sz, st = oracle.ref_phase_draws(seeds, probs, smin, smax, nallocs, PHASE_TRIES,
+                                             niters)
+        index.append({"name": name, "fractions": fr, "probs": probs, "smin": smin,
+                      "smax": smax, "nallocs": nallocs, "niters": niters, "group": group,
+                      "seed": seed, "ntries": PHASE_TRIES})
+        arrays[f"{name}.seeds"] = seeds
+        arrays[f"{name}.ctr"] = ctr.astype(np.uint8)
+        arrays[f"{name}.sizes"] = sz.astype(np.uint16)
+        arrays[f"{name}.states"] = st
+    arrays["index"] = np.frombuffer(json.dumps(index).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "phase_draws.npz"), **arrays)
+
+
 def main():
     if not oracle.reference_available():
         sys.exit("oracle/_ref/libhalloc_refhost.so missing: run make -C oracle ref")
+    what = set(sys.argv[1:]) or {"traces", "phase"}
+    if "phase" in what:
+        phase_draws()
+    if "traces" not in what:
+        return
     with open(os.path.join(HERE, "size_tables.json"), "w") as f:
         json.dump(size_tables(), f, indent=0)
     arrays = {}

@@ -15,8 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
 
 
-def load_golden_traces() -> list:
-    z = np.load(os.path.join(GOLDEN, "traces.npz"))
+def load_golden_traces(fname: str = "traces.npz") -> list:
+    z = np.load(os.path.join(GOLDEN, fname))
     index = json.loads(bytes(z["index"]).decode())
     cases = []
     for e in index:

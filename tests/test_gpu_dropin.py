@@ -32,9 +32,9 @@ def build_dropin_sample(force: bool = False) -> str:
 
 
 def build_new_delete_sample(force: bool = False) -> str:
-    """user_new.cu with -DHALLOC_CPP + libhalloc_cpp.a -> tests/dropin/_build."""
-    from halloc_b200.build import LIB_CPP_A
-    return _build("user_new", LIB_CPP_A, ["-DHALLOC_CPP"], force)
+    """user_new.cu with -DHALLOC_CPP + libhalloc.a -> tests/dropin/_build."""
+    from halloc_b200.build import LIB_A
+    return _build("user_new", LIB_A, ["-DHALLOC_CPP"], force)
 
 
 @pytest.mark.gpu

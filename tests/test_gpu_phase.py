@@ -72,3 +72,85 @@ def test_phase_state_after_alloc_round(torch_cuda):
         a = acc.cpu().numpy()
         assert a[2] == a[3] and a[4] == a[5]
         assert H.stats()["used_chunks"] == 0 and H.status() == 0
+
+
+# ---- the reference's own form (Markov transitions, per-thread generator) ----
+
+def ref_buffers(torch, seeds, n, nallocs):
+    states = torch.tensor(seeds.view(np.int32), device="cuda")
+    slots = torch.zeros(nallocs * n, dtype=torch.int64, device="cuda")
+    ctrs = torch.zeros(n, dtype=torch.int32, device="cuda")
+    acc = torch.zeros(4, dtype=torch.int64, device="cuda")
+    return states, slots, ctrs, acc
+
+
+@pytest.mark.parametrize("group,niters,smax", [(1, 1, 256), (32, 1, 256), (1, 3, 256),
+                                               (1, 1, 4096)])
+def test_phase_ref_tries_match_replay(torch_cuda, group, niters, smax):
+    """Try by try: every thread's block count, which of its slots hold a
+    block, the blocks' validity and the exact slab state equal the replay
+    of the reference's draws (phase-throughput.cu:17-48)."""
+    import halloc_b200
+    from halloc_b200.workloads import group_seeds
+    from oracle.phase import PhaseRefReplay
+    torch = torch_cuda
+    n, nallocs, ntries, smin = 65536, 4, 10, 16
+    probs = halloc_b200.phase_ref_probabilities(0.95, 0.05, 0.91)
+    seeds = group_seeds(n, group, 7 + group)
+    r = PhaseRefReplay(seeds, nallocs, probs, smin, smax, niters)
+    with allocator(memory=1 << 30) as H:
+        states, slots, ctrs, acc = ref_buffers(torch, seeds, n, nallocs)
+        st = H.stats()
+        for t in range(ntries):
+            H.phase_ref_step(n, nallocs, t, niters, probs, smin, smax, states, slots, ctrs, acc)
+            r.step(t)
+            torch.cuda.synchronize()
+            assert np.array_equal(ctrs.cpu().numpy().astype(np.uint32), r.ctr), t
+            p = slots.cpu().numpy()
+            sz = r.sizes.reshape(-1).astype(np.int64)
+            assert np.array_equal(p != 0, sz != 0), t
+            if t in (0, 5, ntries - 1):
+                check_blocks(p, sz, st["pool_base"], st["pool_bytes"], allow_null=True)
+                dump = H.dump_state()
+                counts, bits, nib = expected_slab_state(p, sz, dump["pool_base"], dump["sb_sz"],
+                                                        dump["nsbs"])
+                assert np.array_equal(dump["counters"] >> 12, counts)
+                assert np.array_equal(dump["bits"], bits)
+                assert np.array_equal(nibbles_to_chunk_layout(dump["nibbles"],
+                                                              dump["chunk_enc"]), nib)
+        assert np.array_equal(states.cpu().numpy().view(np.uint32), r.st)
+        a = acc.cpu().numpy()
+        assert a[2] == 0
+        assert a[0] == r.mallocs and a[1] == r.frees and a[3] == r.bytes
+        H.phase_ref_step(n, nallocs, ntries, niters, probs, smin, smax, states, slots, ctrs,
+                         acc, rest=True)
+        r.rest()
+        torch.cuda.synchronize()
+        a = acc.cpu().numpy()
+        assert a[0] == a[1] == r.frees
+        assert not slots.any().item() and not ctrs.any().item()
+        assert H.stats()["used_chunks"] == 0 and H.status() == 0
+
+
+def test_phase_ref_run_readme_config(torch_cuda):
+    """1,048,576 threads x 4 blocks, sizes 16..256, -f0.95 -F0.05 -e0.91,
+    16 tries: the run's counts equal the replay's."""
+    import halloc_b200
+    from halloc_b200.workloads import group_seeds
+    from oracle.phase import PhaseRefReplay
+    torch = torch_cuda
+    n, nallocs, ntries = 1 << 20, 4, 16
+    probs = halloc_b200.phase_ref_probabilities(0.95, 0.05, 0.91)
+    seeds = group_seeds(n, 1, 0x5EED)
+    r = PhaseRefReplay(seeds, nallocs, probs, 16, 256)
+    for t in range(ntries):
+        r.step(t)
+    r.rest()
+    with allocator(memory=1 << 30) as H:
+        states, slots, ctrs, acc = ref_buffers(torch, seeds, n, nallocs)
+        got = H.phase_ref_run(n, nallocs, ntries, 1, probs, 16, 256, states, slots, ctrs, acc)
+        assert got["failed"] == 0
+        assert got["mallocs"] == r.mallocs and got["frees"] == r.frees
+        assert got["bytes"] == r.bytes
+        assert got["kernel_ms"] > 0
+        assert H.stats()["used_chunks"] == 0 and H.status() == 0

@@ -1,6 +1,8 @@
 """The oracle (oracle/ha_model.c) against the reference allocator's own code
 built for the host (oracle/_ref) and against the golden fixtures generated
 from it.  CPU only."""
+import os
+
 import numpy as np
 import pytest
 
@@ -166,3 +168,59 @@ def test_port_and_glibc_plain_runs():
     for kind in ("port", "glibc"):
         dt, cs, nf = oracle.cpu_plain_run(kind, n, iters, 16, 2)
         assert nf == 0 and cs == expect, kind
+
+
+# ---- the reference's phase test: transition probabilities and draws ---------
+
+def test_phase_ref_probabilities():
+    """-f0.95 -F0.05 -e0.91 (halloc README): p00 = p11 = 1.81 / 1.9,
+    p01 = p10 = 0.1 (tst/common/common.cu:311-355, float32)."""
+    from halloc_b200 import HallocError, phase_ref_probabilities
+    p00, p01, p10, p11 = phase_ref_probabilities(0.95, 0.05, 0.91)
+    f32 = np.float32
+    num = f32(0.91) + f32(0.95) - f32(0.05)
+    assert p00 == float(num / (f32(2) * (f32(1) - f32(0.05))))
+    assert p11 == float(num / (f32(2) * f32(0.95)))
+    assert abs(p00 - 0.9526316) < 1e-6 and abs(p01 - 0.1) < 1e-6 and abs(p10 - 0.1) < 1e-6
+    assert phase_ref_probabilities(1.0, 0.0, 1.0) == (1.0, 1.0, 1.0, 1.0)
+    with pytest.raises(HallocError):
+        phase_ref_probabilities(0.9, 0.9, 0.9)   # e + f + F > 2
+    with pytest.raises(HallocError):
+        phase_ref_probabilities(0.9, 0.1, 0.5)   # e < |f - F|
+
+
+def test_wang_hash_vector_and_scalar_agree():
+    from oracle.phase import wang_next, wang_next_scalar
+    x = np.random.default_rng(3).integers(0, 1 << 32, 1000, dtype=np.uint64).astype(np.uint32)
+    assert wang_next(x).tolist() == [wang_next_scalar(int(v)) for v in x]
+
+
+@pytest.mark.parametrize("case", load_golden_traces("phase_draws.npz"),
+                         ids=lambda c: c["name"])
+def test_phase_replay_matches_golden_draws(case):
+    """The host replay's decisions, sizes and generator states equal the
+    reference's own, try by try (fixtures from tst/common/common.h)."""
+    from oracle.phase import PhaseRefReplay
+    r = PhaseRefReplay(case["seeds"], case["nallocs"], case["probs"], case["smin"],
+                       case["smax"], case["niters"])
+    for t in range(case["ntries"]):
+        r.step(t)
+        assert np.array_equal(r.ctr, case["ctr"][t]), t
+        assert np.array_equal(r.sizes, case["sizes"][t]), t
+    assert np.array_equal(r.st, case["states"])
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REF_DRAWS_SO),
+                    reason="reference host build (oracle/_ref) absent")
+def test_phase_replay_matches_reference_draws():
+    from halloc_b200 import phase_ref_probabilities
+    from halloc_b200.workloads import group_seeds
+    from oracle.phase import PhaseRefReplay
+    probs = phase_ref_probabilities(0.9, 0.1, 0.85)
+    seeds = group_seeds(20000, 4, 99)
+    ctr, sz, st = oracle.ref_phase_draws(seeds, probs, 16, 1000, 3, 20, 2)
+    r = PhaseRefReplay(seeds, 3, probs, 16, 1000, 2)
+    for t in range(20):
+        r.step(t)
+        assert np.array_equal(r.ctr, ctr[t]) and np.array_equal(r.sizes, sz[t]), t
+    assert np.array_equal(r.st, st)
