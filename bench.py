@@ -513,7 +513,9 @@ def run_serve(torch, H) -> dict:
     """Serving loop: Poisson arrivals at rate lambda of jobs that grow by 1..32
     blocks of 256 B per step up to ceil(L/256), L log-uniform 64 B..2 MiB,
     and live Exp(mean 50 steps); admission refused while the 12 GiB slab
-    pool of a 16 GiB pool is over 90 % full; one persistent kernel."""
+    pool of a 16 GiB pool is over 90 % full; one persistent kernel of one
+    256-slot block per SM.  The launch with every SM full is reported
+    beside it at the highest rate."""
     H.init(H.HallocOpts(memory=SERVE_POOL))
     out = {"metric": "serving jobs/s and hamalloc latency", "points": []}
     ok = True
@@ -532,30 +534,44 @@ def run_serve(torch, H) -> dict:
             "max_ns": r["max_cycles"] / cpn, "p50_cycles": r["p50_cycles"],
             "p99_cycles": r["p99_cycles"], "sm_ghz": cpn})
         del res
+    # the same at the highest rate, every SM filled with job slots
+    lam, njobs = SERVE_POINTS[-1]
+    res = torch.zeros(2 * njobs, dtype=torch.int64, device="cuda")
+    r = H.serve_run(res, njobs, lam, seed=7, ctas_per_sm=0)
+    cpn = r["cycles_per_ns"] or 1.0
+    ok &= r["jobs_done"] == njobs and r["timeouts"] == 0
+    out["full_occupancy_launch"] = {
+        "lambda": lam, "jobs": njobs, "jobs_per_s": r["jobs_done"] / r["seconds"],
+        "allocs_per_s": r["allocs"] / r["seconds"], "p50_ns": r["p50_cycles"] / cpn,
+        "p99_ns": r["p99_cycles"] / cpn,
+        "note": "as many 256-slot blocks per SM as fit: more warps contend for the "
+                "one head slab of the 256-B size"}
+    del res
     ok &= H.status() == 0 and H.stats()["used_chunks"] == 0
     H.shutdown()
-    # tuned variant: two head slabs per size
-    H.set_heads(2)
+    # tuned variant: four head slabs per size
+    H.set_heads(4)
     H.init(H.HallocOpts(memory=SERVE_POOL))
     H.set_heads(1)
     lam, njobs = SERVE_POINTS[-1]
     res = torch.zeros(2 * njobs, dtype=torch.int64, device="cuda")
     r = H.serve_run(res, njobs, lam, seed=7)
     cpn = r["cycles_per_ns"] or 1.0
-    out["tuned_2_heads"] = {"lambda": lam, "jobs": njobs,
+    out["tuned_4_heads"] = {"lambda": lam, "jobs": njobs,
                             "jobs_per_s": r["jobs_done"] / r["seconds"],
                             "allocs_per_s": r["allocs"] / r["seconds"],
                             "alloc_failures": r["alloc_failures"],
                             "p50_ns": r["p50_cycles"] / cpn, "p99_ns": r["p99_cycles"] / cpn,
                             "ok": r["jobs_done"] == njobs and r["timeouts"] == 0,
-                            "note": "2 head slabs per size (ha_set_heads_c)"}
+                            "note": "4 head slabs per size (ha_set_heads_c)"}
     del res
     H.shutdown()
     out["ok"] = ok
     out["config"] = ("jobs of ceil(L/256) 256-B blocks, L log-uniform 64 B..2 MiB, growing "
                      "1..32 blocks per step, lifetime Exp(mean 50 steps), Poisson arrivals, "
                      "admission refused above 0.9 occupancy of the slab pool (16 GiB pool, "
-                     "12 GiB of slabs), one persistent kernel, host-fed through mapped memory")
+                     "12 GiB of slabs), one persistent kernel of 148 x 256 job slots, host-fed "
+                     "through mapped memory")
     return out
 
 

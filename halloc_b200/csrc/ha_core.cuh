@@ -453,44 +453,64 @@ __device__ __noinline__ uint32_t find_slab(uint32_t sid) {
 // slab is prefetched right away.  One lane per warp calls this.  A caller
 // that loses the race for the size's lock waits (bounded) until the head
 // changes or the lock is released (halloc src/slab.cuh:378-445).
+//
+// The lock covers only the switch of the head.  Filing the old head and
+// prefetching the next slab, which the reference also does under the lock,
+// run after it is released, so other warps can use the new head meanwhile;
+// a single thread still performs the reference's steps in the reference's
+// order.  Two prefetches can then overlap: the loser hands its slab back.
 __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
   // hs = ihead * kNSizes + size id
   const uint32_t sid = hs % kNSizes;
   uint32_t *head = &g_st.head[hs];
   uint32_t *hlock = &g_st.head_lock[hs * kTicketStride];
+  cuda::atomic_ref<uint32_t, cuda::thread_scope_device> cached(g_st.cached[hs]);
   uint32_t seen = ld_relaxed(head);
-  if (try_lock(hlock)) {
+  // test before test-and-set: while the lock is held, waiting warps only read
+  if (ld_relaxed(hlock) == 0 && try_lock(hlock)) {
     uint32_t cur = ld_relaxed(head);
-    uint32_t next;
-    if (cur == kNone || used_of(cur) >= load_class(sid).busy) {
-      next = ld_relaxed(&g_st.cached[hs]);
-      st_relaxed(&g_st.cached[hs], kNone);
-      if (next == kNone) next = find_slab(sid);
-      if (next != kNone) {
-        st_release(head, next);
-        red_add(&g_st.n_head_changes, 1);
-        if (cur != kNone) {
-          if (lock(&g_st.sb_lock[cur])) {
-            detach(cur);
-            unlock(&g_st.sb_lock[cur]);
-          }
-        }
-        st_relaxed(&g_st.cached[hs], find_slab(sid));
-      }
-    } else {
-      next = ld_relaxed(head);
+    if (cur != kNone && used_of(cur) < load_class(sid).busy) {
+      unlock(hlock);
+      return cur;
     }
+    uint32_t next = cached.exchange(kNone, cuda::memory_order_acq_rel);
+    if (next == kNone) next = find_slab(sid);
+    if (next == kNone) {
+      unlock(hlock);
+      return kNone;
+    }
+    st_release(head, next);
+    red_add(&g_st.n_head_changes, 1);
     unlock(hlock);
+    if (cur != kNone) {
+      if (lock(&g_st.sb_lock[cur])) {
+        detach(cur);
+        unlock(&g_st.sb_lock[cur]);
+      }
+    }
+    const uint32_t pre = find_slab(sid);
+    if (pre != kNone) {
+      uint32_t expect = kNone;
+      if (!cached.compare_exchange_strong(expect, pre, cuda::memory_order_acq_rel)) {
+        // another replacement prefetched first: file this slab again
+        if (lock(&g_st.sb_lock[pre])) {
+          detach(pre);
+          unlock(&g_st.sb_lock[pre]);
+        }
+      }
+    }
     return next;
   }
   Deadline dl;
+  uint32_t pause = 64;
   for (;;) {
     if (ld_relaxed(head) != seen || ld_relaxed(hlock) == 0) break;
     if (dl.expired()) {
       raise_status(HA_ST_TIMEOUT);
       return kNone;
     }
-    dl.backoff();
+    __nanosleep(pause);
+    if (pause < 256) pause *= 2;
   }
   return ld_relaxed(head);
 }
