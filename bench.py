@@ -282,6 +282,8 @@ def run_ours(args, rank, world, local_rank):
             res["graph"] = run_leg("graph")
         if not args.skip_serve:
             res["serve"] = run_leg("serve")
+        if not args.skip_samples:
+            res["samples"] = run_leg("samples")
     return res
 
 
@@ -340,6 +342,8 @@ def leg_main(args):
         out = run_serve(torch, H)
     elif args.leg == "atomics":
         out = run_atomic_probe(torch, H)
+    elif args.leg == "samples":
+        out = run_samples(torch, H, 5)
     else:
         out = run_batched(torch, H, 3, not args.no_tune)
     print("LEG " + json.dumps(out), flush=True)
@@ -577,6 +581,84 @@ def run_serve(torch, H) -> dict:
 
 GRAPH_N, GRAPH_POOL = 1 << 20, 1 << 30
 
+SAMPLE_POINTS, SAMPLE_CELLS, SAMPLE_STRINGS, SAMPLE_STRLEN = 1_000_000, 32, 1_000_000, 31
+
+
+def run_samples(torch, H, reps: int) -> dict:
+    """The reference's sample programs at their own sizes (512 MiB pool):
+    grid-points, 1,000,000 points into a 32^3 grid, and add-strings,
+    1,000,000 pairs of 31-character strings concatenated; each kernel timed
+    with CUDA events (median of reps, L2 flushed before each), results
+    checked on the device."""
+    import statistics as stats
+
+    from halloc_b200.workloads import sample_lengths, sample_points
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(fn) -> float:
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    H.init(H.HallocOpts(memory=512 << 20))
+    out = {"config": "samples/grid-points and samples/add-strings at the sizes their main() "
+                     "uses, 512 MiB pool, device time per kernel (median of "
+                     f"{reps}, L2 flushed before each)"}
+    # grid-points
+    n, nc = SAMPLE_POINTS, SAMPLE_CELLS
+    pts = torch.tensor(sample_points(n, seed=5), device="cuda")
+    grid = torch.zeros(nc ** 3, dtype=torch.int64, device="cuda")
+    nodes = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+    nfail = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ins, fre, pre = [], [], []
+    for r in range(reps + 1):
+        t_ins = timed(lambda: H.grid_insert(n, nc, pts, grid, nfail, stream=stream))
+        used = H.stats()["used_chunks"]
+        t_fre = timed(lambda: H.grid_free(nc, grid, stream=stream))
+        t_pre = timed(lambda: H.grid_insert(n, nc, pts, grid, nfail, pre_nodes=nodes,
+                                            stream=stream))
+        H.grid_free(nc, grid, pre_nodes=True, stream=stream)
+        if r:
+            ins.append(t_ins), fre.append(t_fre), pre.append(t_pre)
+    torch.cuda.synchronize()
+    grid_ok = nfail.item() == 0 and used == n and H.stats()["used_chunks"] == 0
+    out["grid_points"] = {
+        "points": n, "cells": nc ** 3,
+        "insert_mpoints_s": n / (stats.median(ins) * 1e-3) / 1e6,
+        "free_mpoints_s": n / (stats.median(fre) * 1e-3) / 1e6,
+        "insert_preallocated_mpoints_s": n / (stats.median(pre) * 1e-3) / 1e6,
+        "insert_ms": stats.median(ins), "free_ms": stats.median(fre), "ok": grid_ok}
+    del pts, grid, nodes
+    # add-strings
+    n = SAMPLE_STRINGS
+    la = torch.full((n,), SAMPLE_STRLEN, dtype=torch.int32, device="cuda")
+    a, b, c = (torch.zeros(n, dtype=torch.int64, device="cuda") for _ in range(3))
+    bad = torch.zeros(1, dtype=torch.int64, device="cuda")
+    t_a, t_c, t_f = [], [], []
+    for r in range(reps + 1):
+        ta = timed(lambda: H.strings_alloc(n, la, a, nfail, stream=stream))
+        ta += timed(lambda: H.strings_alloc(n, la, b, nfail, stream=stream))
+        tc = timed(lambda: H.strings_concat(n, c, a, b, nfail, stream=stream))
+        H.strings_check(n, c, la, la, bad, stream=stream)
+        tf = sum(timed(lambda s=s: H.strings_free(n, s, stream=stream)) for s in (a, b, c))
+        if r:
+            t_a.append(ta / 2), t_c.append(tc), t_f.append(tf / 3)
+    torch.cuda.synchronize()
+    str_ok = nfail.item() == 0 and bad.item() == 0 and H.stats()["used_chunks"] == 0
+    out["add_strings"] = {
+        "strings": n, "length": SAMPLE_STRLEN,
+        "alloc_mstrings_s": n / (stats.median(t_a) * 1e-3) / 1e6,
+        "concat_mstrings_s": n / (stats.median(t_c) * 1e-3) / 1e6,
+        "free_mstrings_s": n / (stats.median(t_f) * 1e-3) / 1e6, "ok": str_ok}
+    out["ok"] = grid_ok and str_ok and H.status() == 0
+    H.shutdown()
+    return out
+
 
 def run_graph(torch, H, reps: int) -> dict:
     """Random-graph build: 1,048,576 vertices, Poisson(16) out-degree from a
@@ -649,6 +731,27 @@ def cpu_sample(kind: str, seconds: float) -> dict:
                       f"{cores} host threads"}
 
 
+def cpu_add_strings() -> dict | None:
+    """The reference's own CPU twin of its add-strings sample
+    (samples/add-strings/add-strings.c, OpenMP over every host core, built
+    unchanged into oracle/_ref): 500,000 strings of 31 characters."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "add_strings_cpu")
+    if not os.path.exists(exe):
+        return None
+    try:
+        p = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    except subprocess.TimeoutExpired:
+        return None
+    out = {"cores": os.cpu_count() or 1, "strings": 500000, "kind": "reference"}
+    for line in p.stdout.splitlines():
+        for key, tag in (("alloc_mstrings_s", "allocation performance"),
+                         ("concat_mstrings_s", "concatenation performance"),
+                         ("free_mstrings_s", "freeing performance")):
+            if tag in line:
+                out[key] = float(line.split(":")[1].split()[0])
+    return out
+
+
 def reference_kind():
     import oracle
     return "reference" if oracle.reference_available() else "port"
@@ -678,6 +781,9 @@ def main_ours(args):
         if cpu:
             cpu["kind"] = kind
         glibc = cpu_sample("glibc", min(3.0, args.cpu_seconds)) if world == 1 else None
+        samples = res.get("samples")
+        if samples is not None and world == 1:
+            samples["add_strings_cpu_baseline"] = cpu_add_strings()
         line = {
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -710,6 +816,7 @@ def main_ours(args):
             "batched": res.get("batched"),
             "graph": res.get("graph"),
             "serve": res.get("serve"),
+            "samples": samples,
             "gpu_launches": args.steps,
             "clocks": res["clocks"],
         }
@@ -765,7 +872,9 @@ def main():
     p.add_argument("--no-tune", action="store_true", help="batched leg without the autotuner")
     p.add_argument("--skip-graph", action="store_true", help="skip the random-graph leg")
     p.add_argument("--skip-serve", action="store_true", help="skip the serving leg")
-    p.add_argument("--leg", choices=["phase", "batched", "graph", "serve", "atomics"],
+    p.add_argument("--skip-samples", action="store_true",
+                   help="skip the grid-points / add-strings sample leg")
+    p.add_argument("--leg", choices=["phase", "batched", "graph", "serve", "atomics", "samples"],
                    help=argparse.SUPPRESS)
     p.add_argument("--only-gpu", action="store_true",
                    help="skip the CPU and CUDA-malloc legs (profiling runs)")

@@ -23,7 +23,9 @@ import numpy as np
 __all__ = [
     "HallocError", "HallocOpts", "init", "shutdown", "extfrag", "stats", "status",
     "clear_status", "set_wait_limit", "dump_state", "l2_persist", "malloc_batch",
-    "free_batch", "phase_round", "phase_run", "phase_ref_step", "phase_ref_run", "graph_build", "graph_gather", "serve_run",
+    "free_batch", "phase_round", "phase_run", "phase_ref_step", "phase_ref_run", "grid_insert",
+    "grid_check", "grid_free", "strings_alloc", "strings_concat", "strings_free",
+    "strings_check", "graph_build", "graph_gather", "serve_run",
     "throughput", "throughput_host", "cuda_throughput", "trace",
     "atomic_peak", "debug_set_head_lock", "set_hash_scale", "set_heads", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
 ]
@@ -148,6 +150,13 @@ _SIGS = {
     "ha_phase_ref_run_c": (_int, [_u32, _u32, _u32, _u32, _vp, _u32, _u32, _vp, _vp, _vp, _vp,
                                   ctypes.POINTER(_CPhaseRefResult), _vp]),
     "ha_atomic_peak_c": (_int, [_vp, _u32, _u32, _u32, _int, _vp]),
+    "ha_grid_insert_c": (_int, [_u32, _u32, _vp, _vp, _vp, _vp, _vp]),
+    "ha_grid_check_c": (_int, [_u32, _vp, _vp, _vp, _vp]),
+    "ha_grid_free_c": (_int, [_u32, _vp, _int, _vp]),
+    "ha_strings_alloc_c": (_int, [_u32, _vp, _vp, _vp, _vp]),
+    "ha_strings_concat_c": (_int, [_u32, _vp, _vp, _vp, _vp, _vp]),
+    "ha_strings_free_c": (_int, [_u32, _vp, _vp]),
+    "ha_strings_check_c": (_int, [_u32, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None
@@ -402,6 +411,44 @@ def phase_ref_probabilities(alloc_fraction: float, free_fraction: float,
     p10 = (e - f + F) / (two * (one - f)) if f < 1 else one
     p11 = (e + f - F) / (two * f) if f > 0 else f32(0)
     return tuple(float(f32(x)) for x in (p00, p01, p10, p11))
+
+
+def grid_insert(n: int, ncells: int, pts, grid, nfail, pre_nodes=None, stream=None) -> None:
+    """grid-points sample: point i (pts: 3 float32 each) gets a 16-byte node,
+    pushed onto its cell of the ncells^3 grid (ha_grid_insert_c)."""
+    _check(load().ha_grid_insert_c(n, ncells, _addr(pts), _addr(grid), _addr(pre_nodes),
+                                   _addr(nfail), _stream(stream)), "ha_grid_insert_c")
+
+
+def grid_check(ncells: int, grid, count, hsum, stream=None) -> None:
+    """Per cell: points and sum of mix32(point index) (ha_grid_check_c)."""
+    _check(load().ha_grid_check_c(ncells, _addr(grid), _addr(count), _addr(hsum),
+                                  _stream(stream)), "ha_grid_check_c")
+
+
+def grid_free(ncells: int, grid, pre_nodes: bool = False, stream=None) -> None:
+    _check(load().ha_grid_free_c(ncells, _addr(grid), int(pre_nodes), _stream(stream)),
+           "ha_grid_free_c")
+
+
+def strings_alloc(n: int, lens, strs, nfail, stream=None) -> None:
+    """add-strings sample: strs[i] = lens[i] spaces (ha_strings_alloc_c)."""
+    _check(load().ha_strings_alloc_c(n, _addr(lens), _addr(strs), _addr(nfail),
+                                     _stream(stream)), "ha_strings_alloc_c")
+
+
+def strings_concat(n: int, c, a, b, nfail, stream=None) -> None:
+    _check(load().ha_strings_concat_c(n, _addr(c), _addr(a), _addr(b), _addr(nfail),
+                                      _stream(stream)), "ha_strings_concat_c")
+
+
+def strings_free(n: int, strs, stream=None) -> None:
+    _check(load().ha_strings_free_c(n, _addr(strs), _stream(stream)), "ha_strings_free_c")
+
+
+def strings_check(n: int, c, la, lb, bad, stream=None) -> None:
+    _check(load().ha_strings_check_c(n, _addr(c), _addr(la), _addr(lb), _addr(bad),
+                                     _stream(stream)), "ha_strings_check_c")
 
 
 def graph_build(n: int, seed: int, cdf, ncdf: int, arr, deg, acc, stream=None) -> None:

@@ -36,7 +36,7 @@ HEADERS = [os.path.join(CSRC, f) for f in ("ha_core.cuh", "ha_types.h")] + [
 # link time, so this bounds the occupancy cost for user kernels (the
 # reference built with the same cap).
 SOURCES = {"halloc.cu": ["-maxrregcount=64"], "ha_kernels.cu": [],
-           "ha_serve.cu": ["-maxrregcount=64"]}
+           "ha_serve.cu": ["-maxrregcount=64"], "ha_samples.cu": []}
 
 
 def nvcc() -> str:

@@ -1,6 +1,6 @@
 """Workload drivers built on the C ABI: the batched request stream, the
-degree table of the random-graph build and the generator seeds of the
-reference-form phase workload.
+degree table of the random-graph build, the generator seeds of the
+reference-form phase workload and the inputs of the sample programs.
 
 The batched stream (64 batches of log-uniform size between 1,024 and
 1,048,576 requests; block sizes geometric over the 16 size classes with
@@ -165,3 +165,20 @@ def group_seeds(nthreads: int, group: int, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     per_group = rng.integers(0, 1 << 31, (nthreads + group - 1) // group, dtype=np.uint32)
     return np.repeat(per_group, group)[:nthreads].astype(np.uint32)
+
+
+def sample_points(n: int, seed: int) -> np.ndarray:
+    """n points in [0, 1)^3 on the 1/65536 lattice of halloc's grid-points
+    sample (samples/grid-points/grid-points.cu:45-54), float32 (n, 3),
+    seeded."""
+    rng = np.random.default_rng(seed)
+    return (rng.integers(0, 65536, (n, 3)) / 65536.0).astype(np.float32)
+
+
+def sample_lengths(n: int, period: int, lo: int, hi: int, seed: int) -> np.ndarray:
+    """String lengths in [lo, hi], equal within groups of `period`
+    consecutive strings, as halloc's add-strings sample draws them
+    (samples/add-strings/add-strings.cu:44-53), seeded."""
+    rng = np.random.default_rng(seed)
+    per = rng.integers(lo, hi + 1, (n + period - 1) // period)
+    return np.repeat(per, period)[:n].astype(np.int32)

@@ -245,6 +245,39 @@ int ha_phase_ref_run_c(uint32_t nthreads, uint32_t nallocs, uint32_t ntries, uin
                        void **slots, uint32_t *ctrs, uint64_t *acc,
                        ha_phase_ref_result_t *res, void *stream);
 
+/* ---- the reference's sample programs ------------------------------ */
+
+/* grid-points (halloc samples/grid-points/grid-points.cu:82-153): point ip
+   of n (pts: device, 3 floats per point in [0, 1]) gets a 16-byte list node,
+   from hamalloc or, when pre_nodes is not NULL, from that device array of n
+   nodes, pushed onto the list of its cell of the ncells^3 grid (grid: device,
+   ncells^3 pointers, NULL at first).  nfail (device, 1 word, accumulated):
+   nodes hamalloc could not give. */
+int ha_grid_insert_c(uint32_t n, uint32_t ncells, const float *pts, void **grid,
+                     void *pre_nodes, uint64_t *nfail, void *stream);
+/* Per cell: the number of points and the sum of mix32(point index) ("lowbias32"
+   finaliser), into device arrays of ncells^3 entries. */
+int ha_grid_check_c(uint32_t ncells, void *const *grid, uint32_t *count, uint64_t *hsum,
+                    void *stream);
+/* One thread per cell frees the cell's nodes (unless pre_nodes) and clears
+   the cell. */
+int ha_grid_free_c(uint32_t ncells, void **grid, int pre_nodes, void *stream);
+
+/* add-strings (halloc samples/add-strings/add-strings.cu:71-205): string i
+   becomes lens[i] spaces and a zero byte in a block from hamalloc
+   (strs: device, n pointers); concat makes c[i] = a[i] followed by b[i] in a
+   new block; free releases and clears every string.  Strings are read and
+   written as 64-bit words.  nfail (device, accumulated): NULL blocks. */
+int ha_strings_alloc_c(uint32_t n, const int *lens, char **strs, uint64_t *nfail,
+                       void *stream);
+int ha_strings_concat_c(uint32_t n, char **c, char *const *a, char *const *b,
+                        uint64_t *nfail, void *stream);
+int ha_strings_free_c(uint32_t n, char **strs, void *stream);
+/* bad (device, accumulated): strings c[i] that are not la[i] + lb[i] spaces
+   and a zero byte. */
+int ha_strings_check_c(uint32_t n, char *const *c, const int *la, const int *lb,
+                       uint64_t *bad, void *stream);
+
 /* ---- batched workload -------------------------------------------- */
 
 /* A stream of allocation batches.  Step s (0 <= s <= nbatch) first frees
