@@ -553,6 +553,37 @@ def run_serve(torch, H) -> dict:
     del res
     ok &= H.status() == 0 and H.stats()["used_chunks"] == 0
     H.shutdown()
+    # the same rate on a growing pool: 1 GiB of the 12 GiB of slabs backed at
+    # init, 1 GiB more whenever the kernel finds none left; trimmed afterwards
+    H.set_growth(1 << 30)
+    try:
+        H.init(H.HallocOpts(memory=SERVE_POOL))
+    finally:
+        H.set_growth(0)
+    res = torch.zeros(2 * njobs, dtype=torch.int64, device="cuda")
+    st0 = H.stats()
+    r = H.serve_run(res, njobs, lam, seed=7, grow_bytes=1 << 30)
+    st1 = H.stats()
+    cpn = r["cycles_per_ns"] or 1.0
+    gok = r["jobs_done"] == njobs and r["timeouts"] == 0 and r["alloc_failures"] == 0
+    released = H.trim()
+    st2 = H.stats()
+    gok &= st1["used_chunks"] == 0 and (H.status() & ~H.ST_GROW) == 0
+    out["growing_pool"] = {
+        "lambda": lam, "jobs": njobs, "jobs_per_s": r["jobs_done"] / r["seconds"],
+        "allocs_per_s": r["allocs"] / r["seconds"], "p50_ns": r["p50_cycles"] / cpn,
+        "p99_ns": r["p99_cycles"] / cpn, "alloc_waits": r["alloc_waits"],
+        "grows": r["grows"], "grow_seconds": r["grow_seconds"],
+        "backed_bytes_start": st0["committed_slabs"] * st0["sb_sz"],
+        "backed_bytes_end": st1["committed_slabs"] * st1["sb_sz"],
+        "released_by_trim": released,
+        "backed_bytes_after_trim": st2["committed_slabs"] * st2["sb_sz"],
+        "slab_pool_bytes": st0["pool_bytes"], "ok": gok,
+        "note": "ha_set_growth_c(1 GiB) + serve grow_bytes 1 GiB: slabs backed by "
+                "cuMemCreate/cuMemMap while the kernel runs, released by ha_trim_c"}
+    ok &= gok
+    del res
+    H.shutdown()
     # tuned variant: four head slabs per size
     H.set_heads(4)
     H.init(H.HallocOpts(memory=SERVE_POOL))

@@ -27,14 +27,15 @@ __all__ = [
     "grid_check", "grid_free", "strings_alloc", "strings_concat", "strings_free",
     "strings_check", "graph_build", "graph_gather", "serve_run",
     "throughput", "throughput_host", "cuda_throughput", "trace",
-    "atomic_peak", "debug_set_head_lock", "set_hash_scale", "set_heads", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
+    "atomic_peak", "debug_set_head_lock", "set_hash_scale", "set_heads", "set_growth", "grow",
+    "trim", "ST_GROW", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
 ]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 SO_PATH = os.path.join(PKG, "libhalloc_b200.so")
 
 HA_OK, HA_EINVAL, HA_ECUDA, HA_ESTATE, HA_ERANGE = 0, -1, -2, -3, -4
-ST_TIMEOUT, ST_BAD_FREE, ST_LIVELOCK = 0x1, 0x2, 0x4
+ST_TIMEOUT, ST_BAD_FREE, ST_LIVELOCK, ST_GROW = 0x1, 0x2, 0x4, 0x8
 NSIZES = 16
 NSETS = 37
 NONE = 0xFFFFFFFF
@@ -75,7 +76,8 @@ class _CStats(ctypes.Structure):
                 ("head_slabs", ctypes.c_uint32), ("status", ctypes.c_uint32),
                 ("n_head_changes", ctypes.c_uint32), ("n_null", ctypes.c_uint32),
                 ("heap_limit_ok", ctypes.c_uint32), ("head", ctypes.c_uint32 * 16),
-                ("cached", ctypes.c_uint32 * 16)]
+                ("cached", ctypes.c_uint32 * 16), ("growth", ctypes.c_uint32),
+                ("committed_slabs", ctypes.c_uint32), ("unit_bytes", ctypes.c_uint64)]
 
 
 class _CPhaseResult(ctypes.Structure):
@@ -95,7 +97,7 @@ class _CServeCfg(ctypes.Structure):
                 ("grow_min", ctypes.c_uint32), ("grow_max", ctypes.c_uint32),
                 ("cta_threads", ctypes.c_uint32), ("ctas_per_sm", ctypes.c_uint32),
                 ("job_ids", ctypes.c_void_p), ("njob_ids", ctypes.c_uint32),
-                ("results", ctypes.c_void_p)]
+                ("results", ctypes.c_void_p), ("grow_bytes", ctypes.c_uint64)]
 
 
 class _CServeResult(ctypes.Structure):
@@ -104,7 +106,9 @@ class _CServeResult(ctypes.Structure):
                 ("alloc_failures", ctypes.c_uint64), ("refusals", ctypes.c_uint64),
                 ("peak_live_blocks", ctypes.c_uint64), ("timeouts", ctypes.c_uint64),
                 ("p50_cycles", ctypes.c_double), ("p99_cycles", ctypes.c_double),
-                ("max_cycles", ctypes.c_double), ("hist", ctypes.c_uint64 * SERVE_HIST)]
+                ("max_cycles", ctypes.c_double), ("hist", ctypes.c_uint64 * SERVE_HIST),
+                ("alloc_waits", ctypes.c_uint64), ("grows", ctypes.c_uint64),
+                ("grown_bytes", ctypes.c_uint64), ("grow_seconds", ctypes.c_double)]
 
 
 class _CPhaseRefResult(ctypes.Structure):
@@ -132,6 +136,9 @@ _SIGS = {
     "ha_debug_set_head_lock_c": (_int, [_u32, _u32]),
     "ha_set_hash_scale_c": (_int, [_u32]),
     "ha_set_heads_c": (_int, [_u32]),
+    "ha_set_growth_c": (_int, [ctypes.c_uint64]),
+    "ha_grow_c": (_int, [ctypes.c_uint64, _vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "ha_trim_c": (_int, [ctypes.c_uint64, _vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ha_serve_run_c": (_int, [ctypes.POINTER(_CServeCfg), ctypes.POINTER(_CServeResult), _vp]),
     "ha_graph_build_c": (_int, [_u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
     "ha_graph_gather_c": (_int, [_u32, _vp, _vp, _vp, _vp, _vp]),
@@ -451,6 +458,32 @@ def strings_check(n: int, c, la, lb, bad, stream=None) -> None:
                                      _stream(stream)), "ha_strings_check_c")
 
 
+def set_growth(initial_bytes: int) -> None:
+    """Applied by the next init on this process: 0 (default) backs the whole
+    slab pool at init; otherwise only initial_bytes, the rest on demand
+    (grow) -- ha_set_growth_c."""
+    _check(load().ha_set_growth_c(initial_bytes), "ha_set_growth_c")
+
+
+def grow(nbytes: int, stream=None) -> int:
+    """Backs at least nbytes more of the slab pool; returns the bytes added
+    (0 when the pool is already fully backed) -- ha_grow_c."""
+    added = ctypes.c_uint64(0)
+    rc = load().ha_grow_c(nbytes, _stream(stream), ctypes.byref(added))
+    if rc == HA_ERANGE:
+        return 0
+    _check(rc, "ha_grow_c")
+    return added.value
+
+
+def trim(max_bytes: int = 1 << 62, stream=None) -> int:
+    """Returns the device memory of wholly free units, up to max_bytes;
+    returns the bytes released -- ha_trim_c."""
+    released = ctypes.c_uint64(0)
+    _check(load().ha_trim_c(max_bytes, _stream(stream), ctypes.byref(released)), "ha_trim_c")
+    return released.value
+
+
 def graph_build(n: int, seed: int, cdf, ncdf: int, arr, deg, acc, stream=None) -> None:
     """Random-graph build with doubling neighbour arrays (ha_graph_build_c)."""
     _check(load().ha_graph_build_c(n, seed, _addr(cdf), ncdf, _addr(arr), _addr(deg),
@@ -467,20 +500,23 @@ def serve_run(results, njobs: int, lam: float, seed: int = 1, occupancy_limit: f
               mean_life: float = 50.0, block_bytes: int = 256, min_len: int = 64,
               max_len: int = 2 << 20, grow_min: int = 1, grow_max: int = 32,
               cta_threads: int = 256, ctas_per_sm: int = 1, job_ids=None,
-              stream=None) -> dict:
+              grow_bytes: int = 0, stream=None) -> dict:
     """Serving loop (ha_serve_run_c).  results: device buffer of 2*njobs
     uint64 (blocks, value sum per job id).  job_ids: optional host sequence
     of ids to release instead of 0..njobs-1.  The default launch, one block
     of 256 job slots per SM, serves 256-B jobs about twice as fast and with
     a several times lower allocation latency than filling every SM: beyond
-    that, more slots only add warps contending for the size's head slab."""
+    that, more slots only add warps contending for the size's head slab.
+    grow_bytes: with a growing pool (set_growth), the kernel asks the host
+    for that much more backed memory whenever a block cannot be had, and the
+    job waits for it instead of failing."""
     ids = None
     if job_ids is not None:
         ids = np.ascontiguousarray(np.asarray(job_ids, dtype=np.uint32))
     cfg = _CServeCfg(njobs, seed, lam, occupancy_limit, mean_life, block_bytes, min_len,
                      max_len, grow_min, grow_max, cta_threads, ctas_per_sm,
                      ids.ctypes.data if ids is not None else None,
-                     len(ids) if ids is not None else 0, _addr(results))
+                     len(ids) if ids is not None else 0, _addr(results), grow_bytes)
     r = _CServeResult()
     _check(load().ha_serve_run_c(ctypes.byref(cfg), ctypes.byref(r), _stream(stream)),
            "ha_serve_run_c")

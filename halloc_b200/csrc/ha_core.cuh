@@ -227,6 +227,7 @@ __device__ __forceinline__ void set_put(uint32_t k, uint32_t sb) {
   red_or(&set_words(k)[w], 1u << (sb & 31));
   fence_acq_rel();
   red_or(&set_sums(k)[w >> 5], 1u << (w & 31));
+  red_add(&g_st.set_epoch, 1u);
 }
 // Clears the summary bit of word w if the word is empty.
 __device__ __forceinline__ void set_tidy(uint32_t k, uint32_t w) {
@@ -239,6 +240,14 @@ __device__ __forceinline__ void set_drop(uint32_t k, uint32_t sb) {
   uint32_t w = sb >> 5, bit = 1u << (sb & 31);
   uint32_t old = atom_and(&set_words(k)[w], ~bit);
   if ((old & ~bit) == 0) set_tidy(k, w);
+}
+// Removes slab sb from set k; false if it was not in the set.
+__device__ __forceinline__ bool set_claim(uint32_t k, uint32_t sb) {
+  uint32_t w = sb >> 5, bit = 1u << (sb & 31);
+  uint32_t old = atom_and(&set_words(k)[w], ~bit);
+  if (!(old & bit)) return false;
+  if ((old & ~bit) == 0) set_tidy(k, w);
+  return true;
 }
 // Removes and returns the lowest slab of set k, or kNone
 // (the search order of halloc src/sbset.cuh:5-35).
@@ -445,6 +454,8 @@ __device__ __noinline__ uint32_t find_slab(uint32_t sid) {
     unlock(&g_st.sb_lock[sb]);
     if (found) return sb;
   }
+  // nothing left; with growth on, tell the host while slabs can still be backed
+  if (c_cfg.growth && ld_relaxed(&g_st.committed) < c_cfg.nsbs) raise_status(HA_ST_GROW);
   return kNone;
 }
 
@@ -466,6 +477,13 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
   uint32_t *hlock = &g_st.head_lock[hs * kTicketStride];
   cuda::atomic_ref<uint32_t, cuda::thread_scope_device> cached(g_st.cached[hs]);
   uint32_t seen = ld_relaxed(head);
+  // A failed search leaves every set it looked at empty, so until a slab is
+  // filed somewhere (set_epoch moves) another search would fail the same
+  // way: answer at once instead of queueing for the lock to search again.
+  const uint32_t epoch = ld_relaxed(&g_st.set_epoch);
+  if (ld_relaxed(&g_st.no_slab[hs]) == epoch + 1u &&
+      (seen == kNone || used_of(seen) >= load_class(sid).busy))
+    return kNone;
   // test before test-and-set: while the lock is held, waiting warps only read
   if (ld_relaxed(hlock) == 0 && try_lock(hlock)) {
     uint32_t cur = ld_relaxed(head);
@@ -476,6 +494,7 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
     uint32_t next = cached.exchange(kNone, cuda::memory_order_acq_rel);
     if (next == kNone) next = find_slab(sid);
     if (next == kNone) {
+      st_relaxed(&g_st.no_slab[hs], epoch + 1u);
       unlock(hlock);
       return kNone;
     }

@@ -25,16 +25,18 @@
 
 namespace {
 
-struct ServeCtl {  // mapped host memory, written by the host
-  uint32_t released;  // ids order[0 .. released) may be claimed
-  uint32_t ended;     // nothing more will be released
+struct ServeCtl {  // mapped host memory
+  uint32_t released;   // host: ids order[0 .. released) may be claimed
+  uint32_t ended;      // host: nothing more will be released
+  uint32_t grow_req;   // device: a block could not be had, back more slabs
+  uint32_t grow_done;  // host: the pool cannot grow any more
 };
 
 struct ServeDev {  // device memory
   uint32_t claimed;        // next index of order[] to hand out
   uint32_t released_seen;  // largest host release count a warp has read
   unsigned long long live_blocks, peak_live;
-  unsigned long long jobs_done, allocs, failures, refusals, timeouts;
+  unsigned long long jobs_done, allocs, failures, refusals, timeouts, waits;
   unsigned long long cycles, nanos;
   unsigned long long hist[HA_SERVE_HIST];
 };
@@ -49,9 +51,14 @@ struct ServeParams {
   uint32_t grow_min, grow_span;
   unsigned long long live_limit;  // admission: live blocks must be <= this
   unsigned long long *results;
-  const ServeCtl *ctl;  // device view of the mapped host struct
+  ServeCtl *ctl;  // device view of the mapped host struct
   ServeDev *dev;
+  uint32_t grow;  // 1: a growing pool, a job waits for memory instead of failing
 };
+
+// steps a job may wait for the pool to grow before its request counts as
+// failed (bounds the kernel when the pool cannot grow in time)
+constexpr uint32_t kMaxStalls = 1u << 16;
 
 __device__ __forceinline__ uint32_t mix32(uint32_t x) {
   x ^= x >> 16;
@@ -81,6 +88,8 @@ __device__ __forceinline__ uint32_t lat_bucket(unsigned long long c) {
 
 struct Job {
   uint32_t id, target, blocks, steps, life, h;
+  uint32_t step_blocks;  // blocks added in the current step
+  uint32_t stalls;       // attempts of the current step that waited for memory
 };
 
 __device__ __forceinline__ void job_start(Job &j, uint32_t id, const ServeParams &P) {
@@ -93,8 +102,13 @@ __device__ __forceinline__ void job_start(Job &j, uint32_t id, const ServeParams
   j.life = max(1u, (uint32_t)ceilf(-P.mean_life * logf(u2)));
   j.blocks = 0;
   j.steps = 0;
+  j.step_blocks = 0;
+  j.stalls = 0;
 }
 
+__device__ __forceinline__ void st_release_sys(uint32_t *p, uint32_t v) {
+  asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
   uint32_t v;
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
@@ -124,7 +138,8 @@ __global__ void __launch_bounds__(1024) ha_serve_k(ServeParams P) {
   j.id = 0xffffffffu;
   bool draining = false;
   void *head = nullptr;
-  unsigned long long vsum = 0, my_allocs = 0, my_fail = 0, my_done = 0, my_refused = 0;
+  unsigned long long vsum = 0, my_allocs = 0, my_fail = 0, my_done = 0, my_refused = 0,
+                     my_waits = 0;
   uint64_t idle_since = 0;
   for (;;) {
     // ---- admission, one claim per warp -------------------------------------
@@ -170,23 +185,37 @@ __global__ void __launch_bounds__(1024) ha_serve_k(ServeParams P) {
       if (!draining) {
         const uint32_t g =
             P.grow_min + mix32(j.h + j.steps * 0x9E3779B9u) % P.grow_span;
-        for (uint32_t i = 0; i < g && j.blocks < j.target; i++) {
+        bool stalled = false;
+        while (j.step_blocks < g && j.blocks < j.target) {
           const long long t0 = clock64();
           void *p = hamalloc(P.block_bytes);
           const long long t1 = clock64();
           atomicAdd(&s_hist[lat_bucket((unsigned long long)(t1 - t0))], 1ull);
           my_allocs++;
           if (!p) {
-            my_fail++;
+            if (P.grow && j.stalls < kMaxStalls && !ld_acquire_sys(&P.ctl->grow_done)) {
+              // ask the host for more slabs; this step resumes later
+              if (!ld_acquire_sys(&P.ctl->grow_req)) st_release_sys(&P.ctl->grow_req, 1u);
+              my_waits++;
+              j.stalls++;
+              stalled = true;
+            } else {
+              my_fail++;
+            }
             break;
           }
           *reinterpret_cast<void **>(p) = head;
           reinterpret_cast<uint32_t *>(p)[2] = mix32(j.id * 0x27D4EB2Fu + j.blocks);
           head = p;
           j.blocks++;
+          j.step_blocks++;
           grown++;
         }
-        if (++j.steps >= j.life) draining = true;
+        if (!stalled) {
+          j.step_blocks = 0;
+          j.stalls = 0;
+          if (++j.steps >= j.life) draining = true;
+        }
       } else {
         for (uint32_t i = 0; i < kDrainPerStep && head; i++) {
           void *nx = *reinterpret_cast<void **>(head);
@@ -242,12 +271,14 @@ __global__ void __launch_bounds__(1024) ha_serve_k(ServeParams P) {
     my_fail += __shfl_down_sync(0xffffffffu, my_fail, o);
     my_done += __shfl_down_sync(0xffffffffu, my_done, o);
     my_refused += __shfl_down_sync(0xffffffffu, my_refused, o);
+    my_waits += __shfl_down_sync(0xffffffffu, my_waits, o);
   }
   if (lane == 0) {
     if (my_allocs) atomicAdd(&P.dev->allocs, my_allocs);
     if (my_fail) atomicAdd(&P.dev->failures, my_fail);
     if (my_done) atomicAdd(&P.dev->jobs_done, my_done);
     if (my_refused) atomicAdd(&P.dev->refusals, my_refused);
+    if (my_waits) atomicAdd(&P.dev->waits, my_waits);
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < HA_SERVE_HIST; i += blockDim.x)
@@ -323,6 +354,8 @@ extern "C" int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out,
   }
   __atomic_store_n(&h_ctl->released, 0u, __ATOMIC_RELEASE);
   __atomic_store_n(&h_ctl->ended, 0u, __ATOMIC_RELEASE);
+  __atomic_store_n(&h_ctl->grow_req, 0u, __ATOMIC_RELEASE);
+  __atomic_store_n(&h_ctl->grow_done, 0u, __ATOMIC_RELEASE);
 
   // Poisson arrival times (seconds from the start)
   std::mt19937_64 rng(cfg->seed * 0x9E3779B97F4A7C15ull + 1);
@@ -358,9 +391,37 @@ extern "C" int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out,
   P.results = reinterpret_cast<unsigned long long *>(cfg->results);
   P.ctl = d_ctl;
   P.dev = d_dev;
+  P.grow = cfg->grow_bytes && st.growth ? 1u : 0u;
+
+  // growth requests are served on a stream of their own while the kernel runs
+  cudaStream_t side = nullptr;
+  if (P.grow && cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess) {
+    cleanup();
+    return HA_ECUDA;
+  }
+  uint64_t grows = 0, grown = 0;
+  double grow_s = 0;
+  auto serve_growth = [&]() {
+    if (!P.grow || !__atomic_load_n(&h_ctl->grow_req, __ATOMIC_ACQUIRE)) return;
+    const auto g0 = std::chrono::steady_clock::now();
+    uint64_t added = 0;
+    int r = ha_grow_c(cfg->grow_bytes, side, &added);
+    // the request stands until the new slabs are in the free set: requests
+    // made meanwhile are the same request
+    if (r == HA_OK && cudaStreamSynchronize(side) != cudaSuccess) r = HA_ECUDA;
+    if (r == HA_OK) {
+      grows++;
+      grown += added;
+    } else {
+      __atomic_store_n(&h_ctl->grow_done, 1u, __ATOMIC_RELEASE);
+    }
+    __atomic_store_n(&h_ctl->grow_req, 0u, __ATOMIC_RELEASE);
+    grow_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - g0).count();
+  };
 
   ha_serve_k<<<nsm * per_sm, cfg->cta_threads, 0, s>>>(P);
   if (cudaGetLastError() != cudaSuccess) {
+    if (side) cudaStreamDestroy(side);
     cleanup();
     return HA_ECUDA;
   }
@@ -376,9 +437,17 @@ extern "C" int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out,
       released = r;
       __atomic_store_n(&h_ctl->released, released, __ATOMIC_RELEASE);
     }
+    serve_growth();
   }
   __atomic_store_n(&h_ctl->ended, 1u, __ATOMIC_RELEASE);
-  const cudaError_t e = cudaStreamSynchronize(s);
+  cudaError_t e;
+  if (P.grow) {
+    while ((e = cudaStreamQuery(s)) == cudaErrorNotReady) serve_growth();
+    if (cudaStreamSynchronize(side) != cudaSuccess) e = cudaErrorUnknown;
+    cudaStreamDestroy(side);
+  } else {
+    e = cudaStreamSynchronize(s);
+  }
   const double secs =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   ServeDev hd;
@@ -396,6 +465,10 @@ extern "C" int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out,
   out->refusals = hd.refusals;
   out->peak_live_blocks = hd.peak_live;
   out->timeouts = hd.timeouts;
+  out->alloc_waits = hd.waits;
+  out->grows = grows;
+  out->grown_bytes = grown;
+  out->grow_seconds = grow_s;
   memcpy(out->hist, hd.hist, sizeof(hd.hist));
   out->p50_cycles = percentile(hd.hist, 0.50);
   out->p99_cycles = percentile(hd.hist, 0.99);

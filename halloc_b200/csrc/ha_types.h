@@ -80,6 +80,7 @@ struct Config {
   uint32_t set_words;     // ceil(nsbs / 32)
   uint32_t sum_words;     // ceil(set_words / 32)
   uint32_t nheads;        // head slabs per size, a power of two <= kMaxHeads
+  uint32_t growth;        // 1: slabs are backed on demand (ha_grow_c)
 };
 
 // mutable allocator state (global memory, one instance per device)
@@ -94,6 +95,11 @@ struct State {
   uint32_t wait_limit_us;
   uint32_t n_head_changes;
   uint32_t n_null;
+  uint32_t committed;     // slabs backed by device memory
+  // bumped by every insertion into a slab set; no_slab[hs] = epoch + 1 when
+  // the last head search for (head, size) hs found nothing at that epoch
+  alignas(128) uint32_t set_epoch;
+  uint32_t no_slab[kMaxHeads * kNSizes];
   alignas(128) uint32_t ctr[kMaxSlabs * kCtrStride];
   Desc desc[kMaxSlabs];
   uint32_t sb_lock[kMaxSlabs];

@@ -6,6 +6,7 @@
 // init / statistics half of the C ABI (halloc_c.h).
 #define HALLOCLIB_COMPILING
 
+#include <cuda.h>  // driver API types; the functions come from cudaGetDriverEntryPoint
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -36,6 +37,11 @@ struct StatsOut {
 };
 __device__ StatsOut g_stats_out;
 __device__ unsigned long long g_max_alloc;
+// ha_trim_c scratch: candidate chunks in (first slab, slab count), the
+// indices of the released ones out
+__device__ uint2 g_trim_chunks[kMaxSlabs];
+__device__ uint32_t g_trim_out[kMaxSlabs];
+__device__ uint32_t g_trim_n, g_trim_slabs;
 }  // namespace ha
 
 // ---------------------------------------------------------------------------
@@ -57,6 +63,8 @@ __device__ __noinline__ void hafree(void *p) {
     free(p);
 }
 
+__global__ void ha_adopt_k(uint32_t first, uint32_t count);
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -73,6 +81,21 @@ struct HostDev {
   uint32_t nsbs, sb_sh;
   bool heap_ok;
   size_t persist_bytes;
+  // growth (ha_set_growth_c): the pool is a reserved address range backed
+  // on demand by chunks, one device allocation each (a handle costs about a
+  // millisecond to create and map whatever its size, so a grow backs its
+  // whole request with one); backed[u] marks the units in a chunk
+  bool growth;
+  unsigned long long va;
+  uint64_t unit_bytes;
+  uint32_t spu;  // slabs per unit
+  uint32_t nunits;
+  uint8_t *backed;
+  struct Chunk {
+    uint32_t first, n;  // units
+    unsigned long long handle;
+  } *chunks;
+  uint32_t nchunks;
 };
 constexpr int kMaxDevices = 64;
 HostDev g_dev[kMaxDevices];
@@ -80,6 +103,8 @@ HostDev g_dev[kMaxDevices];
 uint32_t g_hash_scale_pct = 100;
 // head slabs per size for the next init (1 = the reference policy)
 uint32_t g_nheads = 1;
+// bytes backed at the next init, 0 = the whole pool (no growth)
+uint64_t g_growth_initial = 0;
 
 #define HA_CK(call)                                   \
   do {                                                \
@@ -156,6 +181,111 @@ void build_magics(const ha::Class *cls, uint4 *mod) {
 
 bool valid_fraction(double f) { return f >= 0.0 && f <= 1.0; }
 
+// ---- virtual memory management (driver API through the runtime's entry
+// points, so that the library needs no link against libcuda) --------------
+struct Vmm {
+  CUresult (*reserve)(CUdeviceptr *, size_t, size_t, CUdeviceptr, unsigned long long);
+  CUresult (*free_va)(CUdeviceptr, size_t);
+  CUresult (*create)(CUmemGenericAllocationHandle *, size_t, const CUmemAllocationProp *,
+                     unsigned long long);
+  CUresult (*release)(CUmemGenericAllocationHandle);
+  CUresult (*map)(CUdeviceptr, size_t, size_t, CUmemGenericAllocationHandle,
+                  unsigned long long);
+  CUresult (*unmap)(CUdeviceptr, size_t);
+  CUresult (*set_access)(CUdeviceptr, size_t, const CUmemAccessDesc *, size_t);
+  CUresult (*granularity)(size_t *, const CUmemAllocationProp *,
+                          CUmemAllocationGranularity_flags);
+};
+
+const Vmm *vmm() {
+  static Vmm v;
+  static int state = 0;  // 0 not tried, 1 ok, -1 unavailable
+  if (state == 0) {
+    struct {
+      const char *name;
+      void **fn;
+    } tab[] = {{"cuMemAddressReserve", (void **)&v.reserve},
+               {"cuMemAddressFree", (void **)&v.free_va},
+               {"cuMemCreate", (void **)&v.create},
+               {"cuMemRelease", (void **)&v.release},
+               {"cuMemMap", (void **)&v.map},
+               {"cuMemUnmap", (void **)&v.unmap},
+               {"cuMemSetAccess", (void **)&v.set_access},
+               {"cuMemGetAllocationGranularity", (void **)&v.granularity}};
+    state = 1;
+    for (auto &t : tab) {
+      cudaDriverEntryPointQueryResult q;
+      if (cudaGetDriverEntryPointByVersion(t.name, t.fn, 12000, cudaEnableDefault, &q) !=
+              cudaSuccess ||
+          q != cudaDriverEntryPointSuccess || !*t.fn) {
+        cudaGetLastError();
+        state = -1;
+      }
+    }
+  }
+  return state == 1 ? &v : nullptr;
+}
+
+CUmemAllocationProp unit_prop(int dev) {
+  CUmemAllocationProp p;
+  memset(&p, 0, sizeof(p));
+  p.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+  p.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+  p.location.id = dev;
+  return p;
+}
+
+// Backs units [u, u + n) of h's pool with one allocation; false on a CUDA
+// error (nothing left half done).
+bool back_chunk(HostDev *h, int dev, uint32_t u, uint32_t n) {
+  const Vmm *v = vmm();
+  const CUmemAllocationProp prop = unit_prop(dev);
+  const size_t bytes = (size_t)n * h->unit_bytes;
+  CUmemGenericAllocationHandle hd = 0;
+  if (v->create(&hd, bytes, &prop, 0) != CUDA_SUCCESS) return false;
+  const CUdeviceptr at = (CUdeviceptr)(h->va + (uint64_t)u * h->unit_bytes);
+  if (v->map(at, bytes, 0, hd, 0) != CUDA_SUCCESS) {
+    v->release(hd);
+    return false;
+  }
+  CUmemAccessDesc acc;
+  memset(&acc, 0, sizeof(acc));
+  acc.location = prop.location;
+  acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+  if (v->set_access(at, bytes, &acc, 1) != CUDA_SUCCESS) {
+    v->unmap(at, bytes);
+    v->release(hd);
+    return false;
+  }
+  h->chunks[h->nchunks++] = {u, n, (unsigned long long)hd};
+  memset(h->backed + u, 1, n);
+  return true;
+}
+
+// Unbacks chunk i (the last chunk takes its place in the list).
+void unback_chunk(HostDev *h, uint32_t i) {
+  const Vmm *v = vmm();
+  const HostDev::Chunk c = h->chunks[i];
+  v->unmap((CUdeviceptr)(h->va + (uint64_t)c.first * h->unit_bytes),
+           (size_t)c.n * h->unit_bytes);
+  v->release((CUmemGenericAllocationHandle)c.handle);
+  memset(h->backed + c.first, 0, c.n);
+  h->chunks[i] = h->chunks[--h->nchunks];
+}
+
+// Unbacks every chunk and frees the reserved range.
+void release_pool_range(HostDev *h) {
+  const Vmm *v = vmm();
+  if (!v || !h->va) return;
+  while (h->nchunks) unback_chunk(h, h->nchunks - 1);
+  v->free_va((CUdeviceptr)h->va, (size_t)h->nunits * h->unit_bytes);
+  delete[] h->backed;
+  delete[] h->chunks;
+  h->backed = nullptr;
+  h->chunks = nullptr;
+  h->va = 0;
+}
+
 int shutdown_impl() {
   int dev;
   HostDev *h = current(&dev);
@@ -165,7 +295,10 @@ int shutdown_impl() {
   ha::Config zero;
   memset(&zero, 0, sizeof(zero));
   HA_CK(cudaMemcpyToSymbol(ha::c_cfg, &zero, sizeof(zero)));
-  HA_CK(cudaFree(h->raw_pool));
+  if (h->growth)
+    release_pool_range(h);
+  else
+    HA_CK(cudaFree(h->raw_pool));
   HA_CK(cudaFree(h->meta));
   if (h->persist_bytes) {
     cudaCtxResetPersistingL2Cache();
@@ -209,20 +342,71 @@ int init_impl(const ha_opts_c &o) {
   bool heap_ok = cudaDeviceSetLimit(cudaLimitMallocHeapSize, heap_mem) == cudaSuccess;
   cudaGetLastError();
 
-  char *raw = nullptr;
+  char *raw = nullptr, *pool = nullptr;
   uint32_t *meta = nullptr;
-  const uint64_t pool_bytes = nsbs << sb_sh;
-  if (cudaMalloc(&raw, pool_bytes + sb_bytes) != cudaSuccess) {
-    cudaGetLastError();
-    return HA_ECUDA;
+  // growth: reserve the whole range, back the first units
+  HostDev grow;
+  memset(&grow, 0, sizeof(grow));
+  uint32_t committed = (uint32_t)nsbs;
+  if (g_growth_initial) {
+    const Vmm *v = vmm();
+    if (!v) return HA_ECUDA;
+    const CUmemAllocationProp prop = unit_prop(dev);
+    size_t gran = 0;
+    if (v->granularity(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_MINIMUM) != CUDA_SUCCESS ||
+        gran == 0)
+      return HA_ECUDA;
+    const uint64_t unit = gran > sb_bytes ? gran : sb_bytes;
+    if (unit % gran || unit % sb_bytes) return HA_EINVAL;
+    grow.growth = true;
+    grow.unit_bytes = unit;
+    grow.spu = (uint32_t)(unit >> sb_sh);
+    grow.nunits = (uint32_t)((nsbs << sb_sh) / unit);
+    if (grow.nunits == 0) return HA_EINVAL;
+    nsbs = (uint64_t)grow.nunits * grow.spu;
+    grow.backed = new (std::nothrow) uint8_t[grow.nunits]();
+    grow.chunks = new (std::nothrow) HostDev::Chunk[grow.nunits];
+    if (!grow.backed || !grow.chunks) {
+      delete[] grow.backed;
+      delete[] grow.chunks;
+      return HA_ECUDA;
+    }
+    CUdeviceptr va = 0;
+    if (v->reserve(&va, (size_t)grow.nunits * unit, unit, 0, 0) != CUDA_SUCCESS) {
+      delete[] grow.backed;
+      delete[] grow.chunks;
+      return HA_ECUDA;
+    }
+    grow.va = va;
+    uint64_t want = (g_growth_initial + unit - 1) / unit;
+    if (want > grow.nunits) want = grow.nunits;
+    if (!back_chunk(&grow, dev, 0, (uint32_t)want)) {
+      release_pool_range(&grow);
+      return HA_ECUDA;
+    }
+    committed = (uint32_t)want * grow.spu;
+    pool = (char *)va;
   }
-  char *pool = (char *)(((uintptr_t)raw + sb_bytes - 1) & ~(uintptr_t)(sb_bytes - 1));
+  const uint64_t pool_bytes = nsbs << sb_sh;
+  if (!grow.growth) {
+    if (cudaMalloc(&raw, pool_bytes + sb_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return HA_ECUDA;
+    }
+    pool = (char *)(((uintptr_t)raw + sb_bytes - 1) & ~(uintptr_t)(sb_bytes - 1));
+  }
+  auto free_pool = [&]() {
+    if (grow.growth)
+      release_pool_range(&grow);
+    else
+      cudaFree(raw);
+  };
   const size_t bit_words = (size_t)nsbs << (sb_sh - 9);
   const size_t nib_words = (size_t)nsbs << (sb_sh - 7);
   const size_t meta_bytes = (bit_words + nib_words) * 4;
   if (cudaMalloc(&meta, meta_bytes) != cudaSuccess) {
     cudaGetLastError();
-    cudaFree(raw);
+    free_pool();
     return HA_ECUDA;
   }
   int rc = HA_OK;
@@ -236,10 +420,12 @@ int init_impl(const ha_opts_c &o) {
       st->cached[s] = ha::kNone;
     }
     st->wait_limit_us = ha::kDefaultWaitUs;
+    st->committed = committed;
     for (uint32_t sb = 0; sb < nsbs; sb++) {
       st->ctr[sb * ha::kCtrStride] = ha::kCtrInit;
       st->desc[sb].size_id = ha::kNone;
       st->desc[sb].chunk_id = ha::kNone;
+      if (sb >= committed) continue;  // not backed yet: in no set
       st->sets[ha::kSetFree][sb >> 5] |= 1u << (sb & 31);
       st->sums[ha::kSetFree][sb >> 10] |= 1u << ((sb >> 5) & 31);
     }
@@ -256,6 +442,7 @@ int init_impl(const ha_opts_c &o) {
     cfg.set_words = (uint32_t)((nsbs + 31) / 32);
     cfg.sum_words = (cfg.set_words + 31) / 32;
     cfg.nheads = g_nheads;
+    cfg.growth = grow.growth ? 1 : 0;
     if (cudaMemset(meta, 0, meta_bytes) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_cls, cls, sizeof(cls)) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_mod, mod, sizeof(mod)) != cudaSuccess ||
@@ -268,7 +455,7 @@ int init_impl(const ha_opts_c &o) {
   }
   delete st;
   if (rc != HA_OK) {
-    cudaFree(raw);
+    free_pool();
     cudaFree(meta);
     return rc;
   }
@@ -295,6 +482,21 @@ int init_impl(const ha_opts_c &o) {
   h->sb_sh = sb_sh;
   h->heap_ok = heap_ok;
   h->persist_bytes = persist;
+  if (grow.growth) {
+    // load the adopt kernel now: with lazy module loading its first launch
+    // would otherwise wait for kernels already running, and ha_grow_c is
+    // meant to be called while a persistent kernel waits for the slabs
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, ha_adopt_k) != cudaSuccess) cudaGetLastError();
+  }
+  h->growth = grow.growth;
+  h->va = grow.va;
+  h->unit_bytes = grow.growth ? grow.unit_bytes : pool_bytes;
+  h->spu = grow.spu;
+  h->nunits = grow.nunits;
+  h->backed = grow.backed;
+  h->chunks = grow.chunks;
+  h->nchunks = grow.nchunks;
   return HA_OK;
 }
 
@@ -310,6 +512,51 @@ ha_opts_c to_c(const halloc_opts_t &o) {
 }
 
 }  // namespace
+
+// ---- growth kernels ----------------------------------------------------------
+
+// newly backed slabs [first, first + count) join the free set
+__global__ void ha_adopt_k(uint32_t first, uint32_t count) {
+  using namespace ha;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) set_put(kSetFree, first + i);
+  if (i == 0) red_add(&g_st.committed, count);
+}
+
+// One thread per candidate chunk g_trim_chunks[i] (first slab, slab count):
+// takes every slab of the chunk out of the free set; the chunk is released
+// when all of them were there and are empty, non-head slabs with no chunk
+// size, and when it fits in max_slabs; otherwise the slabs taken go back.
+// Released chunks are listed in g_trim_out[0 .. g_trim_n).
+__global__ void ha_trim_k(uint32_t ncand, uint32_t max_slabs) {
+  using namespace ha;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncand) return;
+  const uint32_t first = g_trim_chunks[i].x, n = g_trim_chunks[i].y;
+  uint32_t taken = 0;
+  bool ok = true;
+  for (; taken < n; taken++)
+    if (!set_claim(kSetFree, first + taken)) {
+      ok = false;
+      break;
+    }
+  for (uint32_t k = 0; k < n && ok; k++) {
+    const uint32_t sb = first + k, c = ld_relaxed(ctr_of(sb));
+    ok = (c >> kCntShift) == 0 && !(c & kHeadFlag) &&
+         ((c >> kChunkShift) & kChunkField) == kChunkField &&
+         !ld_relaxed(&g_st.desc[sb].is_head);
+  }
+  if (ok) {
+    const uint32_t before = atomicAdd(&g_trim_slabs, n);
+    if (before + n <= max_slabs) {
+      g_trim_out[atomicAdd(&g_trim_n, 1u)] = i;
+      red_add(&g_st.committed, 0u - n);
+      return;
+    }
+    atomicSub(&g_trim_slabs, n);
+  }
+  for (uint32_t k = 0; k < taken; k++) set_put(kSetFree, first + k);
+}
 
 // ---- statistics kernels ----------------------------------------------------
 
@@ -434,7 +681,7 @@ extern "C" int ha_stats_c(ha_stats_t *out) {
   ha::StatsOut s;
   int rc = run_stats(0, &s);
   if (rc) return rc;
-  uint32_t head[ha::kNSizes], cached[ha::kNSizes], misc[4];
+  uint32_t head[ha::kNSizes], cached[ha::kNSizes], misc[5];
   HA_CK(cudaMemcpyFromSymbol(head, ha::g_st, sizeof(head), offsetof(ha::State, head)));
   HA_CK(cudaMemcpyFromSymbol(cached, ha::g_st, sizeof(cached), offsetof(ha::State, cached)));
   HA_CK(cudaMemcpyFromSymbol(misc, ha::g_st, sizeof(misc), offsetof(ha::State, status)));
@@ -454,7 +701,113 @@ extern "C" int ha_stats_c(ha_stats_t *out) {
   out->heap_limit_ok = h->heap_ok ? 1 : 0;
   memcpy(out->head, head, sizeof(head));
   memcpy(out->cached, cached, sizeof(cached));
+  out->growth = h->growth ? 1 : 0;
+  out->committed_slabs = misc[4];
+  out->unit_bytes = h->unit_bytes;
   return HA_OK;
+}
+
+extern "C" int ha_set_growth_c(uint64_t initial_bytes) {
+  g_growth_initial = initial_bytes;
+  return HA_OK;
+}
+
+extern "C" int ha_grow_c(uint64_t bytes, void *stream, uint64_t *added_bytes) {
+  if (added_bytes) *added_bytes = 0;
+  int dev;
+  HostDev *h = current(&dev);
+  if (!h) return HA_ECUDA;
+  if (!h->init || !h->growth) return HA_ESTATE;
+  uint64_t want = (bytes + h->unit_bytes - 1) / h->unit_bytes;
+  if (want == 0) want = 1;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  uint64_t added = 0;
+  // lowest unbacked runs first, one chunk per run
+  for (uint32_t u = 0; u < h->nunits && added < want;) {
+    if (h->backed[u]) {
+      u++;
+      continue;
+    }
+    uint32_t n = 0;
+    while (u + n < h->nunits && !h->backed[u + n] && added + n < want) n++;
+    if (!back_chunk(h, dev, u, n)) break;
+    const uint32_t count = n * h->spu;
+    ha_adopt_k<<<(count + 127) / 128, 128, 0, s>>>(u * h->spu, count);
+    if (cudaGetLastError() != cudaSuccess) return HA_ECUDA;
+    added += n;
+    u += n;
+  }
+  if (added_bytes) *added_bytes = added * h->unit_bytes;
+  if (added == 0) {
+    for (uint32_t u = 0; u < h->nunits; u++)
+      if (!h->backed[u]) return HA_ECUDA;  // there was room: a CUDA call failed
+    return HA_ERANGE;
+  }
+  return HA_OK;
+}
+
+extern "C" int ha_trim_c(uint64_t max_bytes, void *stream, uint64_t *released_bytes) {
+  if (released_bytes) *released_bytes = 0;
+  HostDev *h = current();
+  if (!h) return HA_ECUDA;
+  if (!h->init || !h->growth) return HA_ESTATE;
+  const uint64_t max_units = max_bytes / h->unit_bytes;
+  if (max_units == 0 || h->nchunks == 0) return HA_OK;
+  const uint64_t max_slabs64 = max_units * h->spu;
+  const uint32_t max_slabs = max_slabs64 > 0xffffffffull ? 0xffffffffu : (uint32_t)max_slabs64;
+  const uint32_t ncand = h->nchunks;
+  uint2 *cand = new (std::nothrow) uint2[ncand];
+  uint32_t *out = new (std::nothrow) uint32_t[ncand];
+  if (!cand || !out) {
+    delete[] cand;
+    delete[] out;
+    return HA_ECUDA;
+  }
+  for (uint32_t i = 0; i < ncand; i++)
+    cand[i] = make_uint2(h->chunks[i].first * h->spu, h->chunks[i].n * h->spu);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  uint32_t zero2[2] = {0, 0}, n = 0;
+  int rc = HA_OK;
+  if (cudaMemcpyToSymbolAsync(ha::g_trim_chunks, cand, ncand * sizeof(uint2), 0,
+                              cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyToSymbolAsync(ha::g_trim_n, &zero2[0], sizeof(uint32_t), 0,
+                              cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyToSymbolAsync(ha::g_trim_slabs, &zero2[1], sizeof(uint32_t), 0,
+                              cudaMemcpyHostToDevice, s) != cudaSuccess)
+    rc = HA_ECUDA;
+  if (rc == HA_OK) {
+    ha_trim_k<<<(ncand + 127) / 128, 128, 0, s>>>(ncand, max_slabs);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyFromSymbolAsync(&n, ha::g_trim_n, sizeof(n), 0, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      rc = HA_ECUDA;
+  }
+  if (rc == HA_OK && n) {
+    if (cudaMemcpyFromSymbolAsync(out, ha::g_trim_out, n * sizeof(uint32_t), 0,
+                                  cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      rc = HA_ECUDA;
+    } else {
+      // released chunks by their index in the candidate list; unback the
+      // highest index first so that swapping the last chunk into a freed
+      // place never moves a chunk still to be released
+      uint64_t units = 0;
+      for (uint32_t k = 0; k < n; k++) units += h->chunks[out[k]].n;
+      for (uint32_t a = 0; a < n; a++)
+        for (uint32_t b = a + 1; b < n; b++)
+          if (out[b] > out[a]) {
+            const uint32_t t = out[a];
+            out[a] = out[b];
+            out[b] = t;
+          }
+      for (uint32_t k = 0; k < n; k++) unback_chunk(h, out[k]);
+      if (released_bytes) *released_bytes = units * h->unit_bytes;
+    }
+  }
+  delete[] cand;
+  delete[] out;
+  return rc;
 }
 
 extern "C" uint32_t ha_status_c(void) {

@@ -35,6 +35,8 @@ extern "C" {
 #define HA_ST_TIMEOUT 0x1u  /* a bounded device-side wait gave up */
 #define HA_ST_BAD_FREE 0x2u /* hafree of a pointer that is no live block */
 #define HA_ST_LIVELOCK 0x4u /* a hamalloc exceeded its probe-round bound */
+#define HA_ST_GROW 0x8u     /* no slab was left, but the pool can still grow
+                               (ha_grow_c) */
 
 /* Options: same fields, order and layout as struct halloc_opts_t
    (include/halloc.h; halloc src/halloc.h:15-34). */
@@ -78,6 +80,9 @@ typedef struct ha_stats_t {
   uint32_t heap_limit_ok;   /* 1 if the CUDA heap size could be set */
   uint32_t head[16];        /* head slab per size class, 0xffffffff none */
   uint32_t cached[16];      /* prefetched next head per size class */
+  uint32_t growth;          /* 1 when the pool grows on demand (ha_set_growth_c) */
+  uint32_t committed_slabs; /* slabs backed by device memory (nsbs without growth) */
+  uint64_t unit_bytes;      /* growth / release unit, a multiple of the slab size */
 } ha_stats_t;
 
 /* Fills *out (synchronises the device).  No counterpart in the reference,
@@ -106,6 +111,34 @@ int ha_dump_state_c(const ha_state_dump_t *out);
 /* Pins the slab metadata (bit arrays, size nibbles) in L2 for kernels
    launched on `stream` (an access-policy window over the metadata). */
 int ha_l2_persist_c(void *stream);
+
+/* ---- slab growth and release ------------------------------------------
+   halloc commits every slab at init and never gives one back (its TODO at
+   src/slab.cuh:371, the unused SB_CUDA flag at src/slab.h:9-12).  With
+   growth on, init reserves the address range of the whole slab pool but
+   backs only the first initial_bytes with device memory (cuMemCreate /
+   cuMemMap, in units of ha_stats_t.unit_bytes); the other slabs join the
+   free set when ha_grow_c backs them, and ha_trim_c gives the memory of
+   wholly free units back.  Addresses, the grid map and the policy are those
+   of the fully committed pool.  When a head slab is needed and none is
+   left while the pool can still grow, hamalloc returns NULL and raises
+   HA_ST_GROW.  Grow and trim may run while kernels allocate; call them
+   from one host thread per device. */
+
+/* Applied by the next init on this process: 0 (the default) commits the
+   whole pool at init; otherwise init backs initial_bytes (at least one
+   unit) and the pool grows on demand. */
+int ha_set_growth_c(uint64_t initial_bytes);
+/* Backs at least `bytes` more of the pool (lowest units first) and adds
+   their slabs to the free set on `stream`; *added_bytes (may be NULL) gets
+   what was added.  HA_ERANGE when the pool is fully backed, HA_ESTATE
+   without growth. */
+int ha_grow_c(uint64_t bytes, void *stream, uint64_t *added_bytes);
+/* Takes wholly free units (every slab in the free set, no chunk in use) out
+   of the free set, up to max_bytes, and returns their device memory to
+   CUDA; synchronises `stream`.  *released_bytes (may be NULL) gets what was
+   released.  HA_ESTATE without growth. */
+int ha_trim_c(uint64_t max_bytes, void *stream, uint64_t *released_bytes);
 
 /* Tuning knob, applied by the next init on this process: the probe hash
    step of each size class is ncib x (largest prime below span) with span =
@@ -391,6 +424,10 @@ typedef struct ha_serve_cfg_t {
   const uint32_t *job_ids; /* host, optional: the ids to release, in order */
   uint32_t njob_ids;
   uint64_t *results;       /* device, 2 words per job id: blocks, value sum */
+  uint64_t grow_bytes;     /* with a growing pool (ha_set_growth_c): bytes
+                              backed per request of the kernel; a job whose
+                              block cannot be had waits for the pool to grow.
+                              0 = never grow during the run */
 } ha_serve_cfg_t;
 
 #define HA_SERVE_HIST 1024 /* histogram buckets: 16 per power of two */
@@ -402,6 +439,9 @@ typedef struct ha_serve_result_t {
   uint64_t timeouts;       /* idle waits that gave up */
   double p50_cycles, p99_cycles, max_cycles;
   uint64_t hist[HA_SERVE_HIST];
+  uint64_t alloc_waits;    /* attempts that waited for the pool to grow */
+  uint64_t grows, grown_bytes;  /* ha_grow_c calls made for the kernel */
+  double grow_seconds;     /* host time in those calls, new slabs adopted */
 } ha_serve_result_t;
 
 int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out,

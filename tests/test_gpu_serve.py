@@ -61,3 +61,39 @@ def test_admission_gate_refuses_and_recovers(torch_cuda):
         assert r["refusals"] > 0
         assert r["jobs_done"] == n and r["alloc_failures"] == 0 and r["timeouts"] == 0
         assert H.stats()["used_chunks"] == 0 and H.status() == 0
+
+
+def test_serving_on_a_growing_pool(torch_cuda):
+    """The pool backs one unit at init and grows on the kernel's requests
+    while the stream runs: every job completes with the same result as on a
+    fully backed pool, nothing fails, the pool grew, and a trim afterwards
+    gives the memory back."""
+    import halloc_b200 as H
+    torch = torch_cuda
+    n = 3000
+    ref = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+    with allocator(memory=1 << 30):
+        r0 = H.serve_run(ref, n, **CFG)
+        assert r0["jobs_done"] == n and r0["alloc_failures"] == 0
+    H.set_growth(8 << 20)
+    try:
+        H.init(H.HallocOpts(memory=1 << 30))
+    finally:
+        H.set_growth(0)
+    try:
+        st0 = H.stats()
+        res = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+        r = H.serve_run(res, n, grow_bytes=16 << 20, **CFG)
+        assert r["jobs_done"] == n and r["alloc_failures"] == 0 and r["timeouts"] == 0
+        assert r["grows"] >= 1 and r["alloc_waits"] >= 1
+        assert r["grown_bytes"] == r["grows"] * (16 << 20)
+        assert torch.equal(res, ref)
+        st = H.stats()
+        assert st["committed_slabs"] > st0["committed_slabs"]
+        assert st["used_chunks"] == 0
+        assert H.status() & ~H.ST_GROW == 0
+        released = H.trim()
+        assert released % st["unit_bytes"] == 0
+        assert H.stats()["committed_slabs"] == st["committed_slabs"] - released // st["sb_sz"]
+    finally:
+        H.shutdown()
