@@ -157,6 +157,7 @@ _SIGS = {
     "ha_phase_ref_run_c": (_int, [_u32, _u32, _u32, _u32, _vp, _u32, _u32, _vp, _vp, _vp, _vp,
                                   ctypes.POINTER(_CPhaseRefResult), _vp]),
     "ha_atomic_peak_c": (_int, [_vp, _u32, _u32, _u32, _int, _vp]),
+    "ha_atomic_peak_strided_c": (_int, [_vp, _u32, _u32, _u32, _u32, _int, _vp]),
     "ha_grid_insert_c": (_int, [_u32, _u32, _vp, _vp, _vp, _vp, _vp]),
     "ha_grid_check_c": (_int, [_u32, _vp, _vp, _vp, _vp]),
     "ha_grid_free_c": (_int, [_u32, _vp, _int, _vp]),
@@ -530,6 +531,9 @@ def trace(ops, n: int, out, stream=None) -> None:
 
 
 def atomic_peak(buf, nwords: int, nthreads: int, reps: int, returning: bool,
-                stream=None) -> None:
-    _check(load().ha_atomic_peak_c(_addr(buf), nwords, nthreads, reps,
-                                   1 if returning else 0, _stream(stream)), "ha_atomic_peak_c")
+                stream=None, stride: int = 1) -> None:
+    """L2 atomic throughput probe (ha_atomic_peak_strided_c): buf holds
+    nwords x stride 32-bit words."""
+    _check(load().ha_atomic_peak_strided_c(_addr(buf), nwords, stride, nthreads, reps,
+                                           1 if returning else 0, _stream(stream)),
+           "ha_atomic_peak_strided_c")

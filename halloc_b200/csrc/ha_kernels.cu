@@ -571,11 +571,12 @@ __global__ void ha_trace_k(const int64_t *ops, int64_t n, int64_t *out) {
   }
 }
 
-// distinct-address 32-bit atomic OR throughput
-__global__ void ha_atomic_peak_k(uint32_t *buf, uint32_t nwords, uint32_t reps,
-                                 int returning) {
+// distinct-address 32-bit atomic OR throughput; thread t works on word
+// (t mod nwords) x stride (stride 8: every thread on its own 32-byte sector)
+__global__ void ha_atomic_peak_k(uint32_t *buf, uint32_t nwords, uint32_t stride,
+                                 uint32_t reps, int returning) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t *w = &buf[t % nwords];
+  uint32_t *w = &buf[(size_t)(t % nwords) * stride];
   if (returning) {
     uint32_t acc0 = 0, acc1 = 0;
     for (uint32_t r = 0; r < reps; r += 2) {
@@ -1033,8 +1034,14 @@ extern "C" int ha_trace_c(const int64_t *ops, int64_t n, int64_t *out, void *str
 
 extern "C" int ha_atomic_peak_c(uint32_t *buf, uint32_t nwords, uint32_t nthreads,
                                 uint32_t reps, int returning, void *stream) {
-  if (!buf || nwords == 0 || nthreads == 0 || reps == 0) return HA_EINVAL;
-  ha_atomic_peak_k<<<blocks_for(nthreads, 256), 256, 0, as_stream(stream)>>>(buf, nwords, reps,
-                                                                            returning);
+  return ha_atomic_peak_strided_c(buf, nwords, 1, nthreads, reps, returning, stream);
+}
+
+extern "C" int ha_atomic_peak_strided_c(uint32_t *buf, uint32_t nwords, uint32_t stride,
+                                        uint32_t nthreads, uint32_t reps, int returning,
+                                        void *stream) {
+  if (!buf || nwords == 0 || stride == 0 || nthreads == 0 || reps == 0) return HA_EINVAL;
+  ha_atomic_peak_k<<<blocks_for(nthreads, 256), 256, 0, as_stream(stream)>>>(
+      buf, nwords, stride, reps, returning);
   return launch_status();
 }

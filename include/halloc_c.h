@@ -460,6 +460,11 @@ int ha_trace_c(const int64_t *ops, int64_t n, int64_t *out, void *stream);
    denominator; no counterpart in the reference. */
 int ha_atomic_peak_c(uint32_t *buf, uint32_t nwords, uint32_t nthreads,
                      uint32_t reps, int returning, void *stream);
+/* The same with thread t on word (t mod nwords) x stride of buf (nwords x
+   stride words): stride 8 puts every thread on a 32-byte sector of its
+   own, as the allocator's hashed bit-array probes land. */
+int ha_atomic_peak_strided_c(uint32_t *buf, uint32_t nwords, uint32_t stride,
+                             uint32_t nthreads, uint32_t reps, int returning, void *stream);
 
 #ifdef __cplusplus
 }
