@@ -639,22 +639,102 @@ extern "C" int ha_cuda_throughput_c(const uint32_t *sizes, uint32_t nbytes, uint
   return throughput(true, sizes, nbytes, nthreads, block, nallocs, niters, out, stream);
 }
 
+// The host-buffer form runs as one CUDA graph (sizes in, counters cleared,
+// the loop, results out), built on the first call and kept while the
+// arguments stay the same: one launch per call instead of four.
+struct HostLoopGraph {
+  int dev;
+  const uint32_t *h_sizes;
+  uint32_t *d_sizes;
+  uint32_t nbytes, nthreads, block, nallocs, niters;
+  uint64_t *d_out, *h_out;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+};
+static HostLoopGraph g_host_loop = {};
+
+static bool same_host_loop(const HostLoopGraph &a, const HostLoopGraph &b) {
+  return a.dev == b.dev && a.h_sizes == b.h_sizes && a.d_sizes == b.d_sizes &&
+         a.nbytes == b.nbytes && a.nthreads == b.nthreads && a.block == b.block &&
+         a.nallocs == b.nallocs && a.niters == b.niters && a.d_out == b.d_out &&
+         a.h_out == b.h_out;
+}
+
+static int build_host_loop(HostLoopGraph &k) {
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return HA_ECUDA;
+  cudaGraphNode_t deps[2];
+  size_t ndeps = 0;
+  bool ok = true;
+  if (k.h_sizes)
+    ok = cudaGraphAddMemcpyNode1D(&deps[ndeps++], g, nullptr, 0, k.d_sizes, k.h_sizes,
+                                  (size_t)k.nthreads * 4, cudaMemcpyHostToDevice) ==
+         cudaSuccess;
+  cudaMemsetParams ms = {};
+  ms.dst = k.d_out;
+  ms.value = 0;
+  ms.elementSize = 4;
+  ms.width = 4;  // two 64-bit counters
+  ms.height = 1;
+  ms.pitch = 0;
+  ok = ok && cudaGraphAddMemsetNode(&deps[ndeps++], g, nullptr, 0, &ms) == cudaSuccess;
+  const uint32_t *sizes = k.h_sizes ? k.d_sizes : nullptr;
+  unsigned long long *o = reinterpret_cast<unsigned long long *>(k.d_out);
+  void *args[] = {(void *)&sizes, (void *)&k.nbytes, (void *)&k.nthreads, (void *)&k.nallocs,
+                  (void *)&k.niters, (void *)&o};
+  cudaKernelNodeParams kp = {};
+  kp.func = reinterpret_cast<void *>(ha_throughput_k<false>);
+  kp.gridDim = dim3(blocks_for(k.nthreads, k.block));
+  kp.blockDim = dim3(k.block);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = args;
+  cudaGraphNode_t kn = nullptr, out = nullptr;
+  ok = ok && cudaGraphAddKernelNode(&kn, g, deps, ndeps, &kp) == cudaSuccess;
+  ok = ok && cudaGraphAddMemcpyNode1D(&out, g, &kn, 1, k.h_out, k.d_out,
+                                      2 * sizeof(uint64_t), cudaMemcpyDeviceToHost) ==
+                 cudaSuccess;
+  cudaGraphExec_t exec = nullptr;
+  ok = ok && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return HA_ECUDA;
+  }
+  k.graph = g;
+  k.exec = exec;
+  return HA_OK;
+}
+
 extern "C" int ha_throughput_host_c(const uint32_t *h_sizes, uint32_t *d_sizes,
                                     uint32_t nbytes, uint32_t nthreads, uint32_t block,
                                     uint32_t nallocs, uint32_t niters, uint64_t *d_out,
                                     uint64_t *h_out, void *stream) {
-  if (!d_out || !h_out || (h_sizes && !d_sizes)) return HA_EINVAL;
+  if (!d_out || !h_out || (h_sizes && !d_sizes) || block == 0 || block > 1024 ||
+      nallocs == 0 || nallocs > kMaxAllocsPerThread)
+    return HA_EINVAL;
+  if (nthreads == 0 || niters == 0) return HA_OK;
+  HostLoopGraph want = {};
+  if (cudaGetDevice(&want.dev) != cudaSuccess) return HA_ECUDA;
+  want.h_sizes = h_sizes;
+  want.d_sizes = d_sizes;
+  want.nbytes = nbytes;
+  want.nthreads = nthreads;
+  want.block = block;
+  want.nallocs = nallocs;
+  want.niters = niters;
+  want.d_out = d_out;
+  want.h_out = h_out;
+  if (!g_host_loop.exec || !same_host_loop(g_host_loop, want)) {
+    if (g_host_loop.exec) {
+      cudaGraphExecDestroy(g_host_loop.exec);
+      cudaGraphDestroy(g_host_loop.graph);
+      g_host_loop.exec = nullptr;
+    }
+    if (build_host_loop(want) != HA_OK) return HA_ECUDA;
+    g_host_loop = want;
+  }
   cudaStream_t s = as_stream(stream);
-  if (h_sizes &&
-      cudaMemcpyAsync(d_sizes, h_sizes, (size_t)nthreads * 4, cudaMemcpyHostToDevice, s) !=
-          cudaSuccess)
-    return HA_ECUDA;
-  if (cudaMemsetAsync(d_out, 0, 2 * sizeof(uint64_t), s) != cudaSuccess) return HA_ECUDA;
-  int rc = throughput(false, h_sizes ? d_sizes : nullptr, nbytes, nthreads, block, nallocs,
-                      niters, d_out, stream);
-  if (rc) return rc;
-  if (cudaMemcpyAsync(h_out, d_out, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s) !=
-          cudaSuccess ||
+  if (cudaGraphLaunch(g_host_loop.exec, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return HA_ECUDA;
   return HA_OK;
