@@ -363,6 +363,7 @@ def leg_main(args):
                                 "note": "4 head slabs per size (ha_set_heads_c); addresses "
                                         "no longer follow the reference policy"}
         out["reference_form"] = run_phase_ref(torch, H)
+        out["reference_form_latency"] = run_phase_ref_latency(torch, H)
     elif args.leg == "graph":
         out = run_graph(torch, H, 3)
     elif args.leg == "serve":
@@ -473,6 +474,48 @@ def run_phase_ref(torch, H) -> dict:
                 "mallocs": r["mallocs"], "ms": r["kernel_ms"], "ok": ok,
                 "published_kepler_mpairs_s": published[0 if form == "private" else 1],
                 "published_source": src}
+    return out
+
+
+# The reference's latency experiment (tst/exp/scaling/exp-run.pl:56-89):
+# phase-latency -f0.95 -F0.05 -e0.91 -m512MiB -g5 -n<threads> -l1 -s<size>
+# -i16 -t8; published Kepler malloc / free (min, avg, max) cycles from
+# tst/exp/scaling/exp-log-lat.csv:2,3,42,43
+PHASE_LAT_CASES = [
+    (1, 16, ((2669, 3046.49, 5233), (1966, 2053.32, 2606)), "exp-log-lat.csv:2"),
+    (1, 256, ((2664, 3020.17, 5285), (1970, 2051.83, 2578)), "exp-log-lat.csv:3"),
+    (1 << 20, 16, ((2805, 3629.24, 14415), (2130, 2455.04, 5298)), "exp-log-lat.csv:42"),
+    (1 << 20, 256, ((2683, 42801.76, 250025), (2002, 3734.92, 9445)), "exp-log-lat.csv:43"),
+]
+
+
+def run_phase_ref_latency(torch, H) -> dict:
+    """Per-call hamalloc / hafree cycles in the reference's phase-latency
+    experiment, beside the figures halloc published for Kepler."""
+    from halloc_b200.workloads import group_seeds
+    probs = H.phase_ref_probabilities(0.95, 0.05, 0.91)
+    out = {"config": "phase-latency -f0.95 -F0.05 -e0.91 -m536870912 -g5 -l1 -i16 -t8; "
+                     "clock64() around each call, SM cycles", "cases": []}
+    for n, size, published, src in PHASE_LAT_CASES:
+        H.init(H.HallocOpts(memory=512 << 20))
+        seeds = group_seeds(n, 32, 0x5EED)
+        states = torch.tensor(seeds.view(np.int32), device="cuda")
+        slots = torch.zeros(n, dtype=torch.int64, device="cuda")
+        ctrs = torch.zeros(n, dtype=torch.int32, device="cuda")
+        acc = torch.zeros(4, dtype=torch.int64, device="cuda")
+        H.phase_ref_latency(n, 1, 1, 16, probs, size, size, states, slots, ctrs, acc)  # warm-up
+        states.copy_(torch.tensor(seeds.view(np.int32), device="cuda"))
+        lat = H.phase_ref_latency(n, 1, 8, 16, probs, size, size, states, slots, ctrs, acc)
+        ok = H.status() == 0 and H.stats()["used_chunks"] == 0 and acc[2].item() == 0
+        H.shutdown()
+        case = {"threads": n, "size": size, "ok": ok}
+        for k, pub in zip(("malloc", "free"), published):
+            s = lat[k]
+            case[k] = {"n": s["n"], "min": s["min_cycles"], "avg": s["avg_cycles"],
+                       "max": s["max_cycles"], "p50": s["p50_cycles"], "p99": s["p99_cycles"],
+                       "published_kepler_min_avg_max": pub}
+        case["published_source"] = "tst/exp/scaling/" + src
+        out["cases"].append(case)
     return out
 
 

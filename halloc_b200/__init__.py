@@ -23,7 +23,7 @@ import numpy as np
 __all__ = [
     "HallocError", "HallocOpts", "init", "shutdown", "extfrag", "stats", "status",
     "clear_status", "set_wait_limit", "dump_state", "l2_persist", "malloc_batch",
-    "free_batch", "phase_round", "phase_run", "phase_ref_step", "phase_ref_run", "grid_insert",
+    "free_batch", "phase_round", "phase_run", "phase_ref_step", "phase_ref_run", "phase_ref_latency", "grid_insert",
     "grid_check", "grid_free", "strings_alloc", "strings_concat", "strings_free",
     "strings_check", "graph_build", "graph_gather", "serve_run",
     "throughput", "throughput_host", "cuda_throughput", "trace",
@@ -116,6 +116,12 @@ class _CPhaseRefResult(ctypes.Structure):
                 ("free_phase_ms", ctypes.c_double), ("acc", ctypes.c_uint64 * 4)]
 
 
+class _CLatency(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("min_cycles", ctypes.c_double),
+                ("avg_cycles", ctypes.c_double), ("max_cycles", ctypes.c_double),
+                ("p50_cycles", ctypes.c_double), ("p99_cycles", ctypes.c_double)]
+
+
 class _CDump(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in (
         "tickets", "heads", "cached", "size_infos", "counters", "size_id", "chunk_id",
@@ -157,6 +163,8 @@ _SIGS = {
     "ha_phase_ref_run_c": (_int, [_u32, _u32, _u32, _u32, _vp, _u32, _u32, _vp, _vp, _vp, _vp,
                                   ctypes.POINTER(_CPhaseRefResult), _vp]),
     "ha_atomic_peak_c": (_int, [_vp, _u32, _u32, _u32, _int, _vp]),
+    "ha_phase_ref_latency_c": (_int, [_u32, _u32, _u32, _u32, _vp, _u32, _u32, _vp, _vp, _vp,
+                                      _vp, _vp, _vp]),
     "ha_atomic_peak_strided_c": (_int, [_vp, _u32, _u32, _u32, _u32, _int, _vp]),
     "ha_grid_insert_c": (_int, [_u32, _u32, _vp, _vp, _vp, _vp, _vp]),
     "ha_grid_check_c": (_int, [_u32, _vp, _vp, _vp, _vp]),
@@ -401,6 +409,20 @@ def phase_ref_run(nthreads: int, nallocs: int, ntries: int, niters: int, probs, 
            "free_phase_ms": r.free_phase_ms}
     out.update(dict(zip(PHASE_REF_ACC, list(r.acc))))
     return out
+
+
+def phase_ref_latency(nthreads: int, nallocs: int, ntries: int, niters: int, probs,
+                      smin: int, smax: int, states, slots, ctrs, acc, stream=None) -> dict:
+    """The reference's phase-latency test (ha_phase_ref_latency_c): per-call
+    cycles of hamalloc and hafree over ntries tries, then the final free."""
+    out = (_CLatency * 2)()
+    _check(load().ha_phase_ref_latency_c(nthreads, nallocs, ntries, niters, _probs(probs),
+                                         smin, smax, _addr(states), _addr(slots), _addr(ctrs),
+                                         _addr(acc), ctypes.cast(out, ctypes.c_void_p),
+                                         _stream(stream)), "ha_phase_ref_latency_c")
+    f = [k for k, _ in _CLatency._fields_]
+    return {"malloc": {k: getattr(out[0], k) for k in f},
+            "free": {k: getattr(out[1], k) for k in f}}
 
 
 def phase_ref_probabilities(alloc_fraction: float, free_fraction: float,

@@ -29,7 +29,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler", "-fPIC",
                   "-I" + INCLUDE, "-I" + CSRC]
 
-HEADERS = [os.path.join(CSRC, f) for f in ("ha_core.cuh", "ha_types.h")] + [
+HEADERS = [os.path.join(CSRC, f) for f in ("ha_core.cuh", "ha_types.h", "ha_hist.cuh")] + [
     os.path.join(INCLUDE, f) for f in ("halloc.h", "halloc_c.h")]
 # The allocator's device functions are capped at 64 registers: every kernel
 # that calls hamalloc/hafree inherits the callee's register count at device

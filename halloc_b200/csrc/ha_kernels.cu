@@ -9,10 +9,12 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <new>
 #include <vector>
 
 #include "halloc.h"
 #include "halloc_c.h"
+#include "ha_hist.cuh"
 
 namespace {
 
@@ -270,11 +272,39 @@ struct PhaseRefProbs {
   float p[4];  // [phase * 2 + holding]
 };
 
-// acc: [0] mallocs, [1] frees, [2] failed mallocs, [3] bytes of successful mallocs
+// per-call cycles of the timed form: [0] hamalloc, [1] hafree
+struct LatAcc {
+  unsigned long long n[2], sum[2], min[2], max[2];
+  unsigned long long hist[2][ha::kHistBuckets];
+};
+
+// acc: [0] mallocs, [1] frees, [2] failed mallocs, [3] bytes of successful mallocs.
+// kTime: clock64() around every hamalloc / hafree call (the reference's
+// phase-latency kernel, tst/perf/phase-latency/phase-latency.cu:18-56), the
+// cycles filed in block-local histograms and added to *lat at the end.
+template <bool kTime>
 __global__ void ha_phase_ref_k(uint32_t n, uint32_t nallocs, uint32_t step0, uint32_t niters,
                                PhaseRefProbs pr, uint32_t smin, uint32_t smax,
                                uint32_t *states, void **slots, uint32_t *ctrs,
-                               unsigned long long *acc, int rest) {
+                               unsigned long long *acc, int rest, LatAcc *lat) {
+  __shared__ unsigned long long s_hist[kTime ? 2 * ha::kHistBuckets : 1];
+  __shared__ unsigned long long s_n[2], s_sum[2], s_min[2], s_max[2];
+  if (kTime) {
+    for (uint32_t k = threadIdx.x; k < 2 * ha::kHistBuckets; k += blockDim.x) s_hist[k] = 0;
+    if (threadIdx.x < 2) {
+      s_n[threadIdx.x] = s_sum[threadIdx.x] = s_max[threadIdx.x] = 0;
+      s_min[threadIdx.x] = ~0ull;
+    }
+    __syncthreads();
+  }
+  auto file = [&](int kind, long long t0, long long t1) {
+    const unsigned long long c = (unsigned long long)(t1 - t0);
+    atomicAdd(&s_hist[kind * ha::kHistBuckets + ha::lat_bucket(c)], 1ull);
+    atomicAdd(&s_n[kind], 1ull);
+    atomicAdd(&s_sum[kind], c);
+    atomicMin(&s_min[kind], c);
+    atomicMax(&s_max[kind], c);
+  };
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long nmal = 0, nfree = 0, nfail = 0, bytes = 0;
   if (i < n) {
@@ -295,7 +325,9 @@ __global__ void ha_phase_ref_k(uint32_t n, uint32_t nallocs, uint32_t step0, uin
         if (!holding) {
           for (uint32_t k = 0; k < nallocs; k++) {
             const uint32_t sz = smin == smax ? smin : draw_in(st, smin, smax);
+            const long long t0 = kTime ? clock64() : 0;
             void *p = hamalloc(sz);
+            if (kTime) file(0, t0, clock64());
             slots[(size_t)k * n + i] = p;
             if (p) {
               nmal++;
@@ -307,7 +339,9 @@ __global__ void ha_phase_ref_k(uint32_t n, uint32_t nallocs, uint32_t step0, uin
           ctr = nallocs;
         } else {
           for (uint32_t k = 0; k < nallocs; k++) {
+            const long long t0 = kTime ? clock64() : 0;
             hafree(slots[(size_t)k * n + i]);
+            if (kTime) file(1, t0, clock64());
             slots[(size_t)k * n + i] = nullptr;
           }
           nfree += nallocs;
@@ -320,6 +354,17 @@ __global__ void ha_phase_ref_k(uint32_t n, uint32_t nallocs, uint32_t step0, uin
   }
   block_add2(nmal, nfree, acc, acc + 1);
   block_add2(nfail, bytes, acc + 2, acc + 3);
+  if (kTime) {
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < 2 * ha::kHistBuckets; k += blockDim.x)
+      if (s_hist[k]) atomicAdd(&lat->hist[k / ha::kHistBuckets][k % ha::kHistBuckets], s_hist[k]);
+    if (threadIdx.x < 2 && s_n[threadIdx.x]) {
+      atomicAdd(&lat->n[threadIdx.x], s_n[threadIdx.x]);
+      atomicAdd(&lat->sum[threadIdx.x], s_sum[threadIdx.x]);
+      atomicMin(&lat->min[threadIdx.x], s_min[threadIdx.x]);
+      atomicMax(&lat->max[threadIdx.x], s_max[threadIdx.x]);
+    }
+  }
 }
 
 // ---- batched workload ---------------------------------------------------------
@@ -824,10 +869,63 @@ extern "C" int ha_phase_ref_step_c(uint32_t nthreads, uint32_t nallocs, uint32_t
   PhaseRefProbs pr;
   for (int k = 0; k < 4; k++) pr.p[k] = probs[k];
   const uint64_t step0 = (uint64_t)itry * niters;
-  ha_phase_ref_k<<<blocks_for(nthreads, 128), 128, 0, as_stream(stream)>>>(
+  ha_phase_ref_k<false><<<blocks_for(nthreads, 128), 128, 0, as_stream(stream)>>>(
       nthreads, nallocs, (uint32_t)step0, niters, pr, smin, smax, states, slots, ctrs,
-      reinterpret_cast<unsigned long long *>(acc), rest);
+      reinterpret_cast<unsigned long long *>(acc), rest, nullptr);
   return launch_status();
+}
+
+extern "C" int ha_phase_ref_latency_c(uint32_t nthreads, uint32_t nallocs, uint32_t ntries,
+                                      uint32_t niters, const float *probs, uint32_t smin,
+                                      uint32_t smax, uint32_t *states, void **slots,
+                                      uint32_t *ctrs, uint64_t *acc, ha_latency_stats_t *out,
+                                      void *stream) {
+  if (!out || !acc || !probs || !states || !slots || !ctrs || nallocs == 0 ||
+      nallocs > kMaxAllocsPerThread || smin == 0 || smin > smax)
+    return HA_EINVAL;
+  memset(out, 0, 2 * sizeof(*out));
+  if (nthreads == 0) return HA_OK;
+  cudaStream_t s = as_stream(stream);
+  LatAcc *d_lat = nullptr;
+  LatAcc *h_lat = new (std::nothrow) LatAcc;
+  if (!h_lat) return HA_ECUDA;
+  memset(h_lat, 0, sizeof(*h_lat));
+  h_lat->min[0] = h_lat->min[1] = ~0ull;
+  int rc = HA_OK;
+  if (cudaMalloc(&d_lat, sizeof(LatAcc)) != cudaSuccess ||
+      cudaMemcpyAsync(d_lat, h_lat, sizeof(LatAcc), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemsetAsync(acc, 0, 4 * sizeof(uint64_t), s) != cudaSuccess)
+    rc = HA_ECUDA;
+  PhaseRefProbs pr;
+  for (int k = 0; k < 4; k++) pr.p[k] = probs[k];
+  for (uint32_t t = 0; t < ntries && rc == HA_OK; t++) {
+    ha_phase_ref_k<true><<<blocks_for(nthreads, 128), 128, 0, s>>>(
+        nthreads, nallocs, t * niters, niters, pr, smin, smax, states, slots, ctrs,
+        reinterpret_cast<unsigned long long *>(acc), 0, d_lat);
+    rc = launch_status();
+  }
+  if (rc == HA_OK)
+    rc = ha_phase_ref_step_c(nthreads, nallocs, ntries, niters, probs, smin, smax, states,
+                             slots, ctrs, acc, 1, stream);
+  if (rc == HA_OK &&
+      (cudaMemcpyAsync(h_lat, d_lat, sizeof(LatAcc), cudaMemcpyDeviceToHost, s) !=
+           cudaSuccess ||
+       cudaStreamSynchronize(s) != cudaSuccess))
+    rc = HA_ECUDA;
+  if (rc == HA_OK) {
+    for (int k = 0; k < 2; k++) {
+      out[k].n = h_lat->n[k];
+      if (!h_lat->n[k]) continue;
+      out[k].min_cycles = (double)h_lat->min[k];
+      out[k].max_cycles = (double)h_lat->max[k];
+      out[k].avg_cycles = (double)h_lat->sum[k] / (double)h_lat->n[k];
+      out[k].p50_cycles = ha::percentile(h_lat->hist[k], 0.50);
+      out[k].p99_cycles = ha::percentile(h_lat->hist[k], 0.99);
+    }
+  }
+  cudaFree(d_lat);
+  delete h_lat;
+  return rc;
 }
 
 extern "C" int ha_phase_ref_run_c(uint32_t nthreads, uint32_t nallocs, uint32_t ntries,

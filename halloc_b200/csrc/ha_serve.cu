@@ -22,8 +22,13 @@
 
 #include "halloc.h"
 #include "halloc_c.h"
+#include "ha_hist.cuh"
 
 namespace {
+
+using ha::bucket_value;
+using ha::lat_bucket;
+using ha::percentile;
 
 struct ServeCtl {  // mapped host memory
   uint32_t released;   // host: ids order[0 .. released) may be claimed
@@ -79,12 +84,6 @@ __device__ __forceinline__ uint64_t now_ns() {
   return t;
 }
 // log-linear latency bucket: 16 buckets per power of two
-__device__ __forceinline__ uint32_t lat_bucket(unsigned long long c) {
-  if (c < 16) return (uint32_t)c;
-  const uint32_t e = 63 - __clzll(c);
-  const uint32_t b = (e - 3) * 16 + (uint32_t)((c >> (e - 4)) & 15);
-  return b < HA_SERVE_HIST ? b : HA_SERVE_HIST - 1;
-}
 
 struct Job {
   uint32_t id, target, blocks, steps, life, h;
@@ -287,29 +286,6 @@ __global__ void __launch_bounds__(1024) ha_serve_k(ServeParams P) {
     atomicAdd(&P.dev->cycles, (unsigned long long)(clock64() - cyc0));
     atomicAdd(&P.dev->nanos, (unsigned long long)(now_ns() - ns0));
   }
-}
-
-// lower bound of a histogram bucket, in cycles
-double bucket_value(uint32_t b) {
-  if (b < 16) return b;
-  const uint32_t e = b / 16 + 3, m = b % 16;
-  return (double)((16ull + m) << (e - 4));
-}
-
-double percentile(const unsigned long long *h, double q) {
-  unsigned long long total = 0;
-  for (int i = 0; i < HA_SERVE_HIST; i++) total += h[i];
-  if (!total) return 0;
-  const double want = q * (double)total;
-  unsigned long long run = 0;
-  for (int i = 0; i < HA_SERVE_HIST; i++) {
-    run += h[i];
-    if ((double)run >= want) {
-      // midpoint of the bucket
-      return 0.5 * (bucket_value(i) + bucket_value(i + 1));
-    }
-  }
-  return bucket_value(HA_SERVE_HIST - 1);
 }
 
 }  // namespace

@@ -278,6 +278,22 @@ int ha_phase_ref_run_c(uint32_t nthreads, uint32_t nallocs, uint32_t ntries, uin
                        void **slots, uint32_t *ctrs, uint64_t *acc,
                        ha_phase_ref_result_t *res, void *stream);
 
+/* Per-call latency, in SM clock cycles (clock64). */
+typedef struct ha_latency_stats_t {
+  uint64_t n;
+  double min_cycles, avg_cycles, max_cycles, p50_cycles, p99_cycles;
+} ha_latency_stats_t;
+
+/* The reference's phase-latency test (halloc
+   tst/perf/phase-latency/phase-latency.cu:18-56): the tries of
+   ha_phase_ref_run_c with clock64() around every hamalloc and hafree
+   call, then the final free (untimed).  out[0] = hamalloc, out[1] = hafree;
+   percentiles from a 16-per-octave histogram. */
+int ha_phase_ref_latency_c(uint32_t nthreads, uint32_t nallocs, uint32_t ntries,
+                           uint32_t niters, const float *probs, uint32_t smin, uint32_t smax,
+                           uint32_t *states, void **slots, uint32_t *ctrs, uint64_t *acc,
+                           ha_latency_stats_t *out, void *stream);
+
 /* ---- the reference's sample programs ------------------------------ */
 
 /* grid-points (halloc samples/grid-points/grid-points.cu:82-153): point ip

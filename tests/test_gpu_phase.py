@@ -160,3 +160,30 @@ def test_phase_ref_run_readme_config(torch_cuda):
         assert got["bytes"] == r.bytes
         assert got["kernel_ms"] > 0
         assert H.stats()["used_chunks"] == 0 and H.status() == 0
+
+
+def test_phase_ref_latency_counts_every_call(torch_cuda):
+    """The timed form files one sample per hamalloc and hafree call of the
+    tries: the counts equal the replay's, and min <= p50 <= p99 <= max."""
+    import halloc_b200
+    from halloc_b200.workloads import group_seeds
+    from oracle.phase import PhaseRefReplay
+    torch = torch_cuda
+    n, nallocs, ntries, niters = 65536, 2, 4, 4
+    probs = halloc_b200.phase_ref_probabilities(0.95, 0.05, 0.91)
+    seeds = group_seeds(n, 32, 5)
+    r = PhaseRefReplay(seeds, nallocs, probs, 16, 256, niters)
+    for t in range(ntries):
+        r.step(t)
+    with allocator(memory=512 << 20) as H:
+        states, slots, ctrs, acc = ref_buffers(torch, seeds, n, nallocs)
+        lat = H.phase_ref_latency(n, nallocs, ntries, niters, probs, 16, 256, states, slots,
+                                  ctrs, acc)
+        assert lat["malloc"]["n"] == r.mallocs and lat["free"]["n"] == r.frees
+        for k in ("malloc", "free"):
+            s = lat[k]
+            assert 0 < s["min_cycles"] <= s["p50_cycles"] <= s["p99_cycles"]
+            assert s["min_cycles"] <= s["avg_cycles"] <= s["max_cycles"]
+            assert s["p99_cycles"] <= 2 * s["max_cycles"]
+        assert not ctrs.any().item()
+        assert H.stats()["used_chunks"] == 0 and H.status() == 0
