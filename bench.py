@@ -298,7 +298,8 @@ def run_ours(args, rank, world, local_rank):
                               "failed_allocs": cnf,
                               "heap_bytes": H.stats()["cuda_heap_bytes"]}
     H.shutdown()
-    if rank == 0 and not args.only_gpu:
+    # the secondary legs are one-GPU workloads: run them with the N=1 line only
+    if rank == 0 and world == 1 and not args.only_gpu:
         if not args.skip_phase:
             res["phase"] = run_leg("phase")
         if not args.skip_batched:
