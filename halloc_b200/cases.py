@@ -1,7 +1,7 @@
 """Small instances of the workload kernels, each launched once, for
 profiling one kernel at a time and as short usage examples:
 
-    python -m halloc_b200.cases phase_ref|batched|graph|samples|all
+    python -m halloc_b200.cases phase_ref|batched|graph|samples|storm|all
 
 Every case holds at most a few hundred MB on the device and checks its
 result the way the tests do (counts, checksums, an empty pool at the end);
@@ -119,7 +119,25 @@ def samples(torch) -> None:
     _done("samples")
 
 
-CASES = {"phase_ref": phase_ref, "batched": batched, "graph": graph, "samples": samples}
+def storm(torch) -> None:
+    """1,048,576 threads each allocating, writing, reading back and freeing
+    one 256-B block, twice (ha_throughput_k): every resident warp contends
+    for the 256-B size's head slab, which fills every 13,680 blocks."""
+    H.init(H.HallocOpts(memory=1 << 30))
+    n = 1 << 20
+    out = torch.zeros(2, dtype=torch.int64, device="cuda")
+    H.throughput(out, n, nbytes=256, block=128, nallocs=1, niters=2)
+    torch.cuda.synchronize()
+    cs, nfail = out.cpu().tolist()
+    # every block holds {t^0, t^1, t^2, t^3} and is read back into the sum
+    t = np.arange(n, dtype=np.int64)
+    if nfail or cs != int(2 * (4 * (t - t % 4) + 6).sum()):
+        raise RuntimeError(f"storm: checksum {cs} failures {nfail}")
+    _done("storm")
+
+
+CASES = {"phase_ref": phase_ref, "batched": batched, "graph": graph, "samples": samples,
+         "storm": storm}
 
 
 def main(argv) -> None:

@@ -580,8 +580,10 @@ __device__ __forceinline__ uint32_t next_probe(uint32_t first, uint32_t round, u
 // atomicOr would have seen, a partly taken block is left unchanged by the
 // reference's OR-and-roll-back, and the count cannot change during the
 // call -- so addresses, try numbers and give-ups are identical.  Under
-// concurrency a stale word only costs one more try.
-constexpr uint32_t kLookahead = 8;
+// concurrency a stale word only costs one more try.  Four positions: eight
+// load more than they save once many warps probe a nearly full head (those
+// loads queue on the same few sectors as the atomics).
+constexpr uint32_t kLookahead = 4;
 __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t mn, uint64_t mh,
                                            uint32_t first, uint32_t block, uint32_t &pos,
                                            uint32_t &round) {
