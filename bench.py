@@ -436,6 +436,10 @@ PHASE_REF_CASES = [
      "tst/exp/speed/exp-log-combi.csv:4"),
     ("single_16x4", 1 << 20, 4, 16, 16, (1401.70, 1220.15),
      "tst/exp/speed/exp-log-single.csv:2"),
+    ("single_16x1", 1 << 20, 1, 16, 16, (1366.76, 940.35),
+     "tst/exp/scaling/exp-log-thru.csv:47"),
+    ("single_256x1", 1 << 20, 1, 256, 256, (190.58, 557.76),
+     "tst/exp/scaling/exp-log-thru.csv:49"),
 ]
 
 
