@@ -168,6 +168,25 @@ def measure_atomic_peak(torch, H, stream) -> dict:
     return out
 
 
+def measure_lone_warp(torch, H, stream, flush) -> float:
+    """Device time of the plain loop run by ONE warp (32 threads, the same
+    10 iterations, L2 flushed before each run): the latency of one thread's
+    chain of dependent round trips, with nothing to contend with."""
+    import statistics as stats
+    out = torch.zeros(2, dtype=torch.int64, device="cuda")
+    times = []
+    for r in range(13):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        H.throughput(out, 32, NBYTES, 32, NALLOCS, NITERS, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        if r >= 3:
+            times.append(e0.elapsed_time(e1) * 1e3)
+    return stats.median(times)
+
+
 def measure_hot_word_rate(torch, H, stream) -> float:
     """Returning 32-bit atomics per second on ONE word, every thread of the
     device hitting it (same-address atomics serialise in their L2 slice)."""
@@ -278,6 +297,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.only_gpu:
         res["peak"] = measure_atomic_peak(torch, H, stream)
         res["hot_word_rate"] = measure_hot_word_rate(torch, H, stream)
+        res["lone_warp_us"] = measure_lone_warp(torch, H, stream, flush)
         # CUDA in-kernel malloc on the same loop
         cout = torch.zeros(2, dtype=torch.int64, device="cuda")
         H.cuda_throughput(cout, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS, stream=stream)
@@ -909,23 +929,28 @@ def cpu_add_strings() -> dict | None:
 
 
 def hot_word_bound(res: dict, pairs_per_s: float) -> dict:
-    """The resource that binds the plain workload: every warp's malloc adds
-    to, and every warp's free subtracts from, the packed counter of the ONE
-    head slab (16-B blocks: 262,144 per slab, the head is never replaced),
-    so 2 same-address atomics per warp-iteration queue on one L2 word; the
-    size's ticket word takes 1 more in another slice.  Floor = those
-    counter atomics / the measured one-word atomic rate."""
-    rate = res.get("hot_word_rate")
-    if not rate:
-        return None
-    warps = NTHREADS // 32
-    ops = 2 * warps * NITERS * NALLOCS
-    floor_s = ops / rate
+    """What bounds the plain workload: each thread's 10 iterations are a
+    chain of dependent L2 round trips (ticket, reservation, count, payload
+    read-back, nibble, count-down), and one warp running the same loop alone
+    (no contention at all) takes nearly as long as the whole 1,024-warp grid.
+    Floor = that lone warp's launch; frac = floor / the grid's launch.  Also
+    given: the one-word atomic floor of the head slab's counter, which every
+    warp's malloc and free hit (2 per warp-iteration)."""
+    lone = res.get("lone_warp_us")
     launch_s = PAIRS_PER_STEP / pairs_per_s
-    return {"resource": "same-address atomics on the head slab's counter word",
-            "ops_per_launch": ops, "rate_gops_measured": rate / 1e9,
-            "floor_us": floor_s * 1e6, "launch_us": launch_s * 1e6,
-            "frac": floor_s / launch_s}
+    out = None
+    if lone:
+        out = {"resource": "latency of one thread's dependent L2 round trips (10 iterations "
+                           "of malloc, 16-B write, read-back, free)",
+               "floor_us": lone, "launch_us": launch_s * 1e6, "frac": lone * 1e-6 / launch_s,
+               "how": "the same kernel run by one warp alone, L2 flushed, CUDA events"}
+    rate = res.get("hot_word_rate")
+    if rate and out is not None:
+        ops = 2 * (NTHREADS // 32) * NITERS * NALLOCS
+        out["head_counter_word"] = {"ops_per_launch": ops, "rate_gops_measured": rate / 1e9,
+                                    "floor_us": ops / rate * 1e6,
+                                    "frac": ops / rate / launch_s}
+    return out
 
 
 def reference_kind():
