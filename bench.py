@@ -473,32 +473,43 @@ def run_phase_ref(torch, H) -> dict:
     out = {"config": "phase-throughput -f0.95 -F0.05 -e0.91 -m536870912 -g5, as the "
                      "reference's speed experiments run it; device time (CUDA events) "
                      "summed over the launches", "probs": probs}
+    def one(n, nallocs, smin, smax, niters, ntries, nheads):
+        H.set_heads(nheads)
+        try:
+            H.init(H.HallocOpts(memory=512 << 20))
+        finally:
+            H.set_heads(1)
+        seeds = group_seeds(n, 32, 0x5EED)
+        states = torch.tensor(seeds.view(np.int32), device="cuda")
+        slots = torch.zeros(nallocs * n, dtype=torch.int64, device="cuda")
+        ctrs = torch.zeros(n, dtype=torch.int32, device="cuda")
+        acc = torch.zeros(4, dtype=torch.int64, device="cuda")
+        H.phase_ref_run(n, nallocs, 4, niters, probs, smin, smax, states, slots, ctrs,
+                        acc)  # warm-up
+        states.copy_(torch.tensor(seeds.view(np.int32), device="cuda"))
+        r = H.phase_ref_run(n, nallocs, ntries, niters, probs, smin, smax, states, slots,
+                            ctrs, acc)
+        ok = (r["failed"] == 0 and r["mallocs"] == r["frees"] and H.status() == 0 and
+              H.stats()["used_chunks"] == 0)
+        H.shutdown()
+        return r, ok
+
     for name, n, nallocs, smin, smax, published, src in PHASE_REF_CASES:
         for form, niters, ntries in (("spree", 1, 512), ("private", 32, 16)):
-            H.init(H.HallocOpts(memory=512 << 20))
-            seeds = group_seeds(n, 32, 0x5EED)
-            states = torch.tensor(seeds.view(np.int32), device="cuda")
-            slots = torch.zeros(nallocs * n, dtype=torch.int64, device="cuda")
-            ctrs = torch.zeros(n, dtype=torch.int32, device="cuda")
-            acc = torch.zeros(4, dtype=torch.int64, device="cuda")
-            H.phase_ref_run(n, nallocs, 4, niters, probs, smin, smax, states, slots, ctrs,
-                            acc)  # warm-up
-            states.copy_(torch.tensor(seeds.view(np.int32), device="cuda"))
-            r = H.phase_ref_run(n, nallocs, ntries, niters, probs, smin, smax, states, slots,
-                                ctrs, acc)
-            ok = (r["failed"] == 0 and r["mallocs"] == r["frees"] and H.status() == 0 and
-                  H.stats()["used_chunks"] == 0)
-            H.shutdown()
+            r, ok = one(n, nallocs, smin, smax, niters, ntries, 1)
             sec = r["kernel_ms"] * 1e-3
             # the reference's own count: 0.5 x threads x blocks x iterations x tries x e
             formula = 0.5 * n * nallocs * niters * ntries * 0.91
+            r4, ok4 = one(n, nallocs, smin, smax, niters, ntries, 4)
             out[f"{name}_{form}"] = {
                 "args": f"-n{n} -l{nallocs} -s{smin} -S{smax} -i{niters} -t{ntries}",
                 "pairs_per_s": r["mallocs"] / sec,
                 "pairs_per_s_reference_formula": formula / sec,
                 "mallocs": r["mallocs"], "ms": r["kernel_ms"], "ok": ok,
                 "published_kepler_mpairs_s": published[0 if form == "private" else 1],
-                "published_source": src}
+                "published_source": src,
+                "tuned_4_heads": {"pairs_per_s": r4["mallocs"] / (r4["kernel_ms"] * 1e-3),
+                                  "ok": ok4}}
     return out
 
 
