@@ -232,3 +232,29 @@ def test_multi_head_variant(torch_cuda, nheads):
             assert H.status() == 0
     finally:
         halloc_b200.set_heads(1)
+
+
+def test_empty_inputs_are_no_ops(torch_cuda):
+    """Zero threads, zero ops, zero points, zero strings: every entry point
+    returns success, touches nothing and leaves the pool empty (the
+    reference's harness launches with n >= 1 only)."""
+    import halloc_b200
+    torch = torch_cuda
+    with allocator(memory=256 << 20) as H:
+        d = torch.zeros(8, dtype=torch.int64, device="cuda")
+        sizes = torch.zeros(1, dtype=torch.int32, device="cuda")
+        H.malloc_batch(sizes, 0, 1, d)
+        H.free_batch(d, 0, 1)
+        H.throughput(d, 0, nbytes=16)
+        H.trace(d, 0, d)
+        H.phase_round(0, 0, 4, 1, 0, 1 << 31, d, sizes, d, sizes, 1)
+        probs = halloc_b200.phase_ref_probabilities(0.95, 0.05, 0.91)
+        H.phase_ref_step(0, 1, 0, 1, probs, 16, 16, sizes, d, sizes, d)
+        pts = torch.zeros(3, dtype=torch.float32, device="cuda")
+        H.grid_insert(0, 8, pts, d, d)
+        H.strings_alloc(0, sizes, d, d)
+        H.strings_free(0, d)
+        torch.cuda.synchronize()
+        assert not d.any().item()
+        st = H.stats()
+        assert st["used_chunks"] == 0 and st["status"] == 0

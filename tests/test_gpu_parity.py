@@ -54,6 +54,11 @@ SMALL = [16, 24, 32, 48, 64, 96, 128, 192, 256]
     # 40 slabs: the CUDA implementation scans the partial set word
     (dict(memory=80 << 20, halloc_fraction=0.5, sb_sz_sh=20),
      dict(n=20000, sizes=[3072, 2048], pfree=0.05, seed=104)),
+    # size-class edges: zero bytes, one byte, either side of the unit
+    # boundaries, the 3 KiB limit and past it
+    (dict(memory=256 << 20),
+     dict(n=20000, sizes=[0, 1, 15, 16, 17, 24, 25, 33, 47, 49, 255, 257, 383, 385, 1025,
+                          3071, 3072, 3073, 4096], pfree=0.35, seed=105)),
 ])
 def test_serial_trace_matches_model(torch_cuda, opts, targs):
     ops = make_trace(**targs)

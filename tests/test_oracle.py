@@ -12,6 +12,8 @@ from tests.trace_gen import make_trace
 
 SMALL = [16, 24, 32, 48, 64, 96, 128, 192, 256]
 ALL = SMALL + [384, 512, 768, 1024, 1536, 2048, 3072]
+EDGES = [0, 1, 15, 16, 17, 24, 25, 33, 47, 49, 255, 257, 383, 385, 1025, 3071, 3072, 3073,
+         4096]
 
 needs_ref = pytest.mark.skipif(not oracle.reference_available(),
                                reason="reference host build (oracle/_ref) absent")
@@ -113,6 +115,9 @@ REF_CASES = [
     # set word, the model follows with ref_scan_whole_words
     (dict(memory=64 << 20, sb_sz_sh=20), dict(n=20000, sizes=[3072], pfree=0.05, seed=18)),
     (dict(memory=40 << 20, sb_sz_sh=20), dict(n=5000, sizes=SMALL, pfree=0.3, seed=19)),
+    # size-class edges: zero bytes, one byte, either side of every unit
+    # boundary up to the 3 KiB limit and past it
+    (dict(memory=256 << 20), dict(n=20000, sizes=EDGES, pfree=0.35, seed=20)),
 ]
 
 
