@@ -258,3 +258,40 @@ def test_empty_inputs_are_no_ops(torch_cuda):
         assert not d.any().item()
         st = H.stats()
         assert st["used_chunks"] == 0 and st["status"] == 0
+
+
+def test_kernels_on_concurrent_streams(torch_cuda):
+    """hamalloc / hafree called at once from kernels of different streams
+    (halloc's README: thread-safe across kernels): two private-throughput
+    loops and a batch allocation run side by side; every checksum holds, the
+    blocks left live are valid and disjoint, and the pool ends empty."""
+    torch = torch_cuda
+    n = 65536
+    rng = np.random.default_rng(21)
+    sizes = rng.choice(SMALL + [512, 3072], n * 2)
+    with allocator(memory=1 << 30) as H:
+        st = H.stats()
+        streams = [torch.cuda.Stream() for _ in range(3)]
+        outs = [torch.zeros(2, dtype=torch.int64, device="cuda") for _ in range(2)]
+        d_sizes = torch.tensor(sizes.astype(np.int32), device="cuda")
+        ptrs = torch.zeros(n * 2, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        for rep in range(3):
+            for o in outs:
+                o.zero_()
+            torch.cuda.synchronize()
+            H.throughput(outs[0], n, nbytes=16, block=128, nallocs=2, niters=4,
+                         stream=streams[0].cuda_stream)
+            H.throughput(outs[1], n, nbytes=96, block=256, nallocs=1, niters=6,
+                         stream=streams[1].cuda_stream)
+            H.malloc_batch(d_sizes, n, 2, ptrs, tag=True, stream=streams[2].cuda_stream)
+            torch.cuda.synchronize()
+            assert outs[0].cpu().tolist() == [plain_checksum(n, 8), 0]
+            assert outs[1].cpu().tolist() == [plain_checksum(n, 6), 0]
+            p = ptrs.cpu().numpy()
+            check_blocks(p, sizes, st["pool_base"], st["pool_bytes"])
+            assert_state_matches_live(H, p, sizes)
+            H.free_batch(ptrs, n, 2, stream=streams[2].cuda_stream)
+            torch.cuda.synchronize()
+            assert_empty(H)
+        assert H.status() == 0
