@@ -16,12 +16,6 @@ def small_plan():
     return batched_plan(seed=3, nbatch=12, max_batch=1 << 15)
 
 
-def test_plan_shape(small_plan):
-    p = small_plan
-    assert p.batch_start[-1] == p.nreq == p.free_start[-1]
-    assert np.array_equal(np.sort(p.free_ids), np.arange(p.nreq, dtype=np.uint32))
-
-
 def test_batched_plain_form(torch_cuda, small_plan):
     from halloc_b200.workloads import BatchedRunner
     torch = torch_cuda

@@ -10,16 +10,6 @@ from tests.helpers import allocator
 pytestmark = pytest.mark.gpu
 
 
-def test_poisson_thresholds_shape():
-    from halloc_b200.workloads import poisson_thresholds
-    t = poisson_thresholds(16.0)
-    assert (np.diff(t.astype(np.int64)) >= 0).all() and t[-1] == 2**32 - 1
-    # mean degree of the table is 16 to within rounding
-    cdf = t.astype(np.float64) / 2**32
-    pmf = np.diff(np.concatenate([[0.0], cdf]))
-    assert abs((pmf * np.arange(len(t))).sum() - 16.0) < 1e-3
-
-
 @pytest.mark.parametrize("n", [1 << 16, 1 << 20])
 def test_graph_build_is_bit_exact(torch_cuda, n):
     import halloc_b200 as H
