@@ -460,6 +460,18 @@ PHASE_REF_CASES = [
      "tst/exp/scaling/exp-log-thru.csv:47"),
     ("single_256x1", 1 << 20, 1, 256, 256, (190.58, 557.76),
      "tst/exp/scaling/exp-log-thru.csv:49"),
+    # the scaling experiment at 1,024 and 32,768 threads (halloc timed these
+    # per launch with the host clock, launch overhead included)
+    ("scaling_16x1_1k", 1024, 1, 16, 16, (89.53, 15.43), "tst/exp/scaling/exp-log-thru.csv:17"),
+    ("scaling_16x4_1k", 1024, 4, 16, 16, (118.87, 45.02), "tst/exp/scaling/exp-log-thru.csv:18"),
+    ("scaling_256x1_1k", 1024, 1, 256, 256, (92.89, 15.51),
+     "tst/exp/scaling/exp-log-thru.csv:19"),
+    ("scaling_16x1_32k", 32768, 1, 16, 16, (1012.49, 347.03),
+     "tst/exp/scaling/exp-log-thru.csv:32"),
+    ("scaling_16x4_32k", 32768, 4, 16, 16, (1218.44, 753.21),
+     "tst/exp/scaling/exp-log-thru.csv:33"),
+    ("scaling_256x1_32k", 32768, 1, 256, 256, (621.78, 312.41),
+     "tst/exp/scaling/exp-log-thru.csv:34"),
 ]
 
 
