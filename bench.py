@@ -517,6 +517,7 @@ def run_phase_ref(torch, H) -> dict:
                 "args": f"-n{n} -l{nallocs} -s{smin} -S{smax} -i{niters} -t{ntries}",
                 "pairs_per_s": r["mallocs"] / sec,
                 "pairs_per_s_reference_formula": formula / sec,
+                "pairs_per_s_wall_per_launch": r["mallocs"] / (r["wall_ms"] * 1e-3),
                 "mallocs": r["mallocs"], "ms": r["kernel_ms"], "ok": ok,
                 "published_kepler_mpairs_s": published[0 if form == "private" else 1],
                 "published_source": src,

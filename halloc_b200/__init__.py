@@ -113,7 +113,8 @@ class _CServeResult(ctypes.Structure):
 
 class _CPhaseRefResult(ctypes.Structure):
     _fields_ = [("kernel_ms", ctypes.c_double), ("alloc_phase_ms", ctypes.c_double),
-                ("free_phase_ms", ctypes.c_double), ("acc", ctypes.c_uint64 * 4)]
+                ("free_phase_ms", ctypes.c_double), ("acc", ctypes.c_uint64 * 4),
+                ("wall_ms", ctypes.c_double)]
 
 
 class _CLatency(ctypes.Structure):
@@ -406,7 +407,7 @@ def phase_ref_run(nthreads: int, nallocs: int, ntries: int, niters: int, probs, 
                                      _addr(acc), ctypes.byref(r), _stream(stream)),
            "ha_phase_ref_run_c")
     out = {"kernel_ms": r.kernel_ms, "alloc_phase_ms": r.alloc_phase_ms,
-           "free_phase_ms": r.free_phase_ms}
+           "free_phase_ms": r.free_phase_ms, "wall_ms": r.wall_ms}
     out.update(dict(zip(PHASE_REF_ACC, list(r.acc))))
     return out
 

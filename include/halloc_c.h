@@ -269,10 +269,13 @@ typedef struct ha_phase_ref_result_t {
   double alloc_phase_ms; /* even tries */
   double free_phase_ms;  /* odd tries and the final free */
   uint64_t acc[4];       /* as in ha_phase_ref_step_c, over the whole run */
+  double wall_ms;        /* host clock around each launch and its
+                            synchronisation, summed (how halloc timed it) */
 } ha_phase_ref_result_t;
 
-/* ntries tries then the final free, each launch timed with CUDA events
-   (the host loop of phase-throughput.cu:76-110).  acc is reset first. */
+/* ntries tries then the final free, each launch timed with CUDA events and
+   waited for (the host loop of phase-throughput.cu:76-110).  acc is reset
+   first. */
 int ha_phase_ref_run_c(uint32_t nthreads, uint32_t nallocs, uint32_t ntries, uint32_t niters,
                        const float *probs, uint32_t smin, uint32_t smax, uint32_t *states,
                        void **slots, uint32_t *ctrs, uint64_t *acc,
