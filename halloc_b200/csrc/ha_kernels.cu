@@ -687,7 +687,9 @@ extern "C" int ha_cuda_throughput_c(const uint32_t *sizes, uint32_t nbytes, uint
 
 // The host-buffer form runs as one CUDA graph (sizes in, counters cleared,
 // the loop, results out), built on the first call and kept while the
-// arguments stay the same: one launch per call instead of four.
+// arguments stay the same: one launch per call instead of four.  The cached
+// graph is one per process: calls from several host threads must not
+// overlap.
 struct HostLoopGraph {
   int dev;
   const uint32_t *h_sizes;

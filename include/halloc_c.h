@@ -191,7 +191,10 @@ int ha_throughput_c(const uint32_t *sizes, uint32_t nbytes, uint32_t nthreads,
 
 /* The same loop end to end from host memory: copies h_sizes (nthreads
    words; NULL for a fixed nbytes) into d_sizes, clears d_out, runs the
-   loop, copies d_out (2 words) to h_out and synchronises the stream. */
+   loop, copies d_out (2 words) to h_out and synchronises the stream.  The
+   four steps run as one CUDA graph, built on the first call and reused
+   while the arguments stay the same (one graph per process: calls from
+   several host threads must not overlap). */
 int ha_throughput_host_c(const uint32_t *h_sizes, uint32_t *d_sizes,
                          uint32_t nbytes, uint32_t nthreads, uint32_t block,
                          uint32_t nallocs, uint32_t niters, uint64_t *d_out,
