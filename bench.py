@@ -625,14 +625,16 @@ def run_batched(torch, H, reps: int, tune: bool) -> dict:
         t["best"]["value"] = n / (t["best"]["ms"] * 1e-3)
         t["best"]["speedup_vs_plain"] = min(plain) / t["best"]["ms"]
         res["autotune"] = t
-    res["small_only"] = run_batched_small_only(torch, H, reps)
+    res["small_only"] = run_batched_small_only(torch, H, reps, tune)
     return res
 
 
-def run_batched_small_only(torch, H, reps: int) -> dict:
+def run_batched_small_only(torch, H, reps: int, tune: bool = False) -> dict:
     """The same stream without its 1 % of large requests (same seed, sizes
     and lifetimes otherwise): what the slabs alone sustain, without CUDA's
-    in-kernel malloc for the 4..64 KiB requests."""
+    in-kernel malloc for the 4..64 KiB requests; then the autotuner on it,
+    where the allocator's own settings decide the time."""
+    from halloc_b200.autotune import autotune
     from halloc_b200.workloads import BatchedRunner, batched_plan
     plan = batched_plan(seed=1, large_frac=0.0)
     runner = BatchedRunner(plan, torch)
@@ -675,6 +677,11 @@ def run_batched_small_only(torch, H, reps: int) -> dict:
         runner.release()
         H.shutdown()
     out["requests"] = plan.nreq
+    if tune and "plain" in out:
+        t = autotune(torch, runner, BATCH_POOL, BATCH_HF, reps=2)
+        t["best"]["value"] = plan.nreq / (t["best"]["ms"] * 1e-3)
+        t["best"]["speedup_vs_plain"] = min(out["plain"]["ms"]) / t["best"]["ms"]
+        out["autotune"] = t
     return out
 
 
