@@ -97,7 +97,8 @@ class _CServeCfg(ctypes.Structure):
                 ("grow_min", ctypes.c_uint32), ("grow_max", ctypes.c_uint32),
                 ("cta_threads", ctypes.c_uint32), ("ctas_per_sm", ctypes.c_uint32),
                 ("job_ids", ctypes.c_void_p), ("njob_ids", ctypes.c_uint32),
-                ("results", ctypes.c_void_p), ("grow_bytes", ctypes.c_uint64)]
+                ("results", ctypes.c_void_p), ("grow_bytes", ctypes.c_uint64),
+                ("prereleased", ctypes.c_uint32)]
 
 
 class _CServeResult(ctypes.Structure):
@@ -524,7 +525,7 @@ def serve_run(results, njobs: int, lam: float, seed: int = 1, occupancy_limit: f
               mean_life: float = 50.0, block_bytes: int = 256, min_len: int = 64,
               max_len: int = 2 << 20, grow_min: int = 1, grow_max: int = 32,
               cta_threads: int = 256, ctas_per_sm: int = 1, job_ids=None,
-              grow_bytes: int = 0, stream=None) -> dict:
+              grow_bytes: int = 0, prereleased: bool = False, stream=None) -> dict:
     """Serving loop (ha_serve_run_c).  results: device buffer of 2*njobs
     uint64 (blocks, value sum per job id).  job_ids: optional host sequence
     of ids to release instead of 0..njobs-1.  The default launch, one block
@@ -533,14 +534,16 @@ def serve_run(results, njobs: int, lam: float, seed: int = 1, occupancy_limit: f
     that, more slots only add warps contending for the size's head slab.
     grow_bytes: with a growing pool (set_growth), the kernel asks the host
     for that much more backed memory whenever a block cannot be had, and the
-    job waits for it instead of failing."""
+    job waits for it instead of failing.  prereleased: every job is handed
+    over before the launch (a closed batch; arrival times are not used)."""
     ids = None
     if job_ids is not None:
         ids = np.ascontiguousarray(np.asarray(job_ids, dtype=np.uint32))
     cfg = _CServeCfg(njobs, seed, lam, occupancy_limit, mean_life, block_bytes, min_len,
                      max_len, grow_min, grow_max, cta_threads, ctas_per_sm,
                      ids.ctypes.data if ids is not None else None,
-                     len(ids) if ids is not None else 0, _addr(results), grow_bytes)
+                     len(ids) if ids is not None else 0, _addr(results), grow_bytes,
+                     1 if prereleased else 0)
     r = _CServeResult()
     _check(load().ha_serve_run_c(ctypes.byref(cfg), ctypes.byref(r), _stream(stream)),
            "ha_serve_run_c")

@@ -1,7 +1,7 @@
 """Small instances of the workload kernels, each launched once, for
 profiling one kernel at a time and as short usage examples:
 
-    python -m halloc_b200.cases phase_ref|batched|graph|samples|storm|all
+    python -m halloc_b200.cases phase_ref|batched|graph|samples|storm|serve|all
 
 Every case holds at most a few hundred MB on the device and checks its
 result the way the tests do (counts, checksums, an empty pool at the end);
@@ -136,8 +136,20 @@ def storm(torch) -> None:
     _done("storm")
 
 
+def serve(torch) -> None:
+    """The serving kernel on a closed batch of 20,000 jobs, all handed over
+    before the launch (ha_serve_k waits on nothing from the host)."""
+    H.init(H.HallocOpts(memory=1 << 30))
+    n = 20000
+    res = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+    r = H.serve_run(res, n, 1e8, seed=7, max_len=64 << 10, prereleased=True)
+    if r["jobs_done"] != n or r["alloc_failures"] or r["timeouts"]:
+        raise RuntimeError(f"serve: {r['jobs_done']} jobs, {r['alloc_failures']} failures")
+    _done("serve")
+
+
 CASES = {"phase_ref": phase_ref, "batched": batched, "graph": graph, "samples": samples,
-         "storm": storm}
+         "storm": storm, "serve": serve}
 
 
 def main(argv) -> None:

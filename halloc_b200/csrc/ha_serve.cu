@@ -332,6 +332,10 @@ extern "C" int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out,
   __atomic_store_n(&h_ctl->ended, 0u, __ATOMIC_RELEASE);
   __atomic_store_n(&h_ctl->grow_req, 0u, __ATOMIC_RELEASE);
   __atomic_store_n(&h_ctl->grow_done, 0u, __ATOMIC_RELEASE);
+  if (cfg->prereleased) {  // a closed batch: every job known before the launch
+    __atomic_store_n(&h_ctl->released, n, __ATOMIC_RELEASE);
+    __atomic_store_n(&h_ctl->ended, 1u, __ATOMIC_RELEASE);
+  }
 
   // Poisson arrival times (seconds from the start)
   std::mt19937_64 rng(cfg->seed * 0x9E3779B97F4A7C15ull + 1);
@@ -403,7 +407,7 @@ extern "C" int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out,
   }
   // release jobs at their arrival times
   const auto t0 = std::chrono::steady_clock::now();
-  uint32_t released = 0;
+  uint32_t released = cfg->prereleased ? n : 0;
   while (released < n) {
     const double now =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -450,6 +450,9 @@ typedef struct ha_serve_cfg_t {
                               backed per request of the kernel; a job whose
                               block cannot be had waits for the pool to grow.
                               0 = never grow during the run */
+  uint32_t prereleased;    /* 1: every job is released (and the stream ended)
+                              before the launch -- a closed batch, and a kernel
+                              that waits on nothing from the host */
 } ha_serve_cfg_t;
 
 #define HA_SERVE_HIST 1024 /* histogram buckets: 16 per power of two */

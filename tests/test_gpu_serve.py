@@ -97,3 +97,20 @@ def test_serving_on_a_growing_pool(torch_cuda):
         assert H.stats()["committed_slabs"] == st["committed_slabs"] - released // st["sb_sz"]
     finally:
         H.shutdown()
+
+
+def test_closed_batch_gives_the_streamed_results(torch_cuda):
+    """All jobs handed over before the launch (prereleased): every job's
+    result equals the streamed run's."""
+    import halloc_b200 as H
+    torch = torch_cuda
+    n = 2000
+    with allocator(memory=1 << 30):
+        a = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+        b = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+        ra = H.serve_run(a, n, **CFG)
+        rb = H.serve_run(b, n, prereleased=True, **CFG)
+        assert ra["jobs_done"] == rb["jobs_done"] == n
+        assert rb["alloc_failures"] == 0 and rb["timeouts"] == 0
+        assert torch.equal(a, b)
+        assert H.stats()["used_chunks"] == 0 and H.status() == 0
