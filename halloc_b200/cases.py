@@ -145,6 +145,8 @@ def serve(torch) -> None:
     r = H.serve_run(res, n, 1e8, seed=7, max_len=64 << 10, prereleased=True)
     if r["jobs_done"] != n or r["alloc_failures"] or r["timeouts"]:
         raise RuntimeError(f"serve: {r['jobs_done']} jobs, {r['alloc_failures']} failures")
+    print(f"serve: {r['seconds'] * 1e3:.2f} ms wall, {r['allocs']} allocations, "
+          f"p50 {r['p50_cycles']:.0f} / p99 {r['p99_cycles']:.0f} cycles per hamalloc")
     _done("serve")
 
 

@@ -150,8 +150,9 @@ __global__ void __launch_bounds__(1024) ha_serve_k(ServeParams P) {
         my_refused++;
       } else {
         uint32_t c = ld_relaxed_u32(&P.dev->claimed);
-        uint32_t r = min(ld_relaxed_u32(&P.dev->released_seen), P.norder);
-        if (r <= c) {  // nothing known to be claimable: look at the host counter
+        // once every job is claimed, neither counter can offer one more
+        uint32_t r = c < P.norder ? min(ld_relaxed_u32(&P.dev->released_seen), P.norder) : c;
+        if (r <= c && c < P.norder) {  // nothing known to be claimable: look at the host counter
           r = min(ld_acquire_sys(&P.ctl->released), P.norder);
           if (r > c) atomicMax(&P.dev->released_seen, r);
         }
