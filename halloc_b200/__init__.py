@@ -154,6 +154,8 @@ _SIGS = {
     "ha_free_batch_c": (_int, [_vp, _u32, _u32, _vp]),
     "ha_throughput_c": (_int, [_vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp]),
     "ha_throughput_host_c": (_int, [_vp, _vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp, _vp]),
+    "ha_throughput_host_ex_c": (_int, [_vp, _vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp, _u32,
+                                       _vp]),
     "ha_cuda_throughput_c": (_int, [_vp, _u32, _u32, _u32, _u32, _u32, _vp, _vp]),
     "ha_trace_c": (_int, [_vp, _i64, _vp, _vp]),
     "ha_phase_round_c": (_int, [_int, _u32, _u32, _u32, _u32, _u32, _vp, _u32, _vp, _vp, _vp,
@@ -339,13 +341,19 @@ def cuda_throughput(out, nthreads: int, nbytes: int = 16, block: int = 128, nall
                                        _addr(out), _stream(stream)), "ha_cuda_throughput_c")
 
 
+XFER_AUTO, XFER_COPY, XFER_MAPPED = 0, 1, 2
+
+
 def throughput_host(h_out: np.ndarray, d_out, nthreads: int, nbytes: int = 16,
                     block: int = 128, nallocs: int = 1, niters: int = 1, h_sizes=None,
-                    d_sizes=None, stream=None) -> None:
-    """End-to-end form: host sizes in, host (checksum, nfail) out."""
-    _check(load().ha_throughput_host_c(_addr(h_sizes), _addr(d_sizes), nbytes, nthreads,
-                                       block, nallocs, niters, _addr(d_out), _addr(h_out),
-                                       _stream(stream)), "ha_throughput_host_c")
+                    d_sizes=None, stream=None, transfer: int = XFER_AUTO) -> None:
+    """End-to-end form: host sizes in, host (checksum, nfail) out.  transfer:
+    XFER_AUTO (mapped when both host buffers are pinned), XFER_COPY (copy
+    engine, one cached CUDA graph) or XFER_MAPPED (the kernel reads the sizes
+    and stores the totals through the pinned buffers)."""
+    _check(load().ha_throughput_host_ex_c(_addr(h_sizes), _addr(d_sizes), nbytes, nthreads,
+                                          block, nallocs, niters, _addr(d_out), _addr(h_out),
+                                          transfer, _stream(stream)), "ha_throughput_host_ex_c")
 
 
 def phase_round(kind: int, nthreads: int, nslots: int, seed: int, round_id: int, thr: int,

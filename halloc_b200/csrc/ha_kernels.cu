@@ -110,39 +110,75 @@ __global__ void ha_free_batch_k(void *const *ptrs, uint32_t n, uint32_t nallocs)
 }
 
 // throughput_malloc_free_k of halloc tst/perf/priv-throughput/priv-throughput.cu:13-27,
-// with the 16-byte payload write and checksummed read-back of each block
+// with the 16-byte payload write and checksummed read-back of each block:
+// one thread's loop, adding its checksum and failed allocations to sum / nfail
+template <bool kCudaHeap>
+__device__ __forceinline__ void throughput_thread(uint32_t i, uint32_t sz, uint32_t nallocs,
+                                                  uint32_t niters, unsigned long long &sum,
+                                                  unsigned long long &nfail) {
+  const uint4 word = make_uint4(i ^ 0u, i ^ 1u, i ^ 2u, i ^ 3u);
+  void *ps[kMaxAllocsPerThread];
+  for (uint32_t it = 0; it < niters; it++) {
+    for (uint32_t a = 0; a < nallocs; a++) {
+      void *p = kCudaHeap ? malloc(sz) : hamalloc(sz);
+      ps[a] = p;
+      if (p)
+        store16(p, word);
+      else
+        nfail++;
+    }
+    for (uint32_t a = 0; a < nallocs; a++) {
+      void *p = ps[a];
+      if (!p) continue;
+      const uint4 v = load16(p);
+      sum += (unsigned long long)v.x + v.y + v.z + v.w;
+      if (kCudaHeap)
+        free(p);
+      else
+        hafree(p);
+    }
+  }
+}
+
 template <bool kCudaHeap>
 __global__ void ha_throughput_k(const uint32_t *sizes, uint32_t nbytes, uint32_t n,
                                 uint32_t nallocs, uint32_t niters,
                                 unsigned long long *out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long sum = 0, nfail = 0;
-  if (i < n) {
-    const uint32_t sz = sizes ? sizes[i] : nbytes;
-    const uint4 word = make_uint4(i ^ 0u, i ^ 1u, i ^ 2u, i ^ 3u);
-    void *ps[kMaxAllocsPerThread];
-    for (uint32_t it = 0; it < niters; it++) {
-      for (uint32_t a = 0; a < nallocs; a++) {
-        void *p = kCudaHeap ? malloc(sz) : hamalloc(sz);
-        ps[a] = p;
-        if (p)
-          store16(p, word);
-        else
-          nfail++;
-      }
-      for (uint32_t a = 0; a < nallocs; a++) {
-        void *p = ps[a];
-        if (!p) continue;
-        const uint4 v = load16(p);
-        sum += (unsigned long long)v.x + v.y + v.z + v.w;
-        if (kCudaHeap)
-          free(p);
-        else
-          hafree(p);
-      }
+  if (i < n) throughput_thread<kCudaHeap>(i, sizes ? sizes[i] : nbytes, nallocs, niters, sum, nfail);
+  block_add2(sum, nfail, out, out + 1);
+}
+
+// Totals of the mapped-transfer loop while its blocks run; the last block
+// to finish takes them (and clears them for the next launch).
+__device__ unsigned long long g_mapped_acc[2];
+__device__ unsigned int g_mapped_done;
+
+// The same loop for the host-buffer form with mapped transfers: sizes is a
+// device view of pinned host memory (read in place over the bus, NULL for a
+// fixed nbytes), and the block that finishes last stores the totals into
+// d_out and into h_out, a device view of the pinned host result.
+__global__ void ha_throughput_mapped_k(const uint32_t *sizes, uint32_t nbytes, uint32_t n,
+                                       uint32_t nallocs, uint32_t niters,
+                                       unsigned long long *d_out, unsigned long long *h_out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long sum = 0, nfail = 0;
+  if (i < n) throughput_thread<false>(i, sizes ? sizes[i] : nbytes, nallocs, niters, sum, nfail);
+  block_add2(sum, nfail, g_mapped_acc, g_mapped_acc + 1);  // thread 0 adds the block's totals
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&g_mapped_done, 1u) == gridDim.x - 1) {
+      __threadfence();
+      const unsigned long long cs = atomicExch(&g_mapped_acc[0], 0ull);
+      const unsigned long long nf = atomicExch(&g_mapped_acc[1], 0ull);
+      g_mapped_done = 0;
+      d_out[0] = cs;
+      d_out[1] = nf;
+      h_out[0] = cs;
+      h_out[1] = nf;
     }
   }
-  block_add2(sum, nfail, out, out + 1);
 }
 
 // ---- phase workload ----------------------------------------------------------
@@ -685,11 +721,14 @@ extern "C" int ha_cuda_throughput_c(const uint32_t *sizes, uint32_t nbytes, uint
   return throughput(true, sizes, nbytes, nthreads, block, nallocs, niters, out, stream);
 }
 
-// The host-buffer form runs as one CUDA graph (sizes in, counters cleared,
-// the loop, results out), built on the first call and kept while the
-// arguments stay the same: one launch per call instead of four.  The cached
-// graph is one per process: calls from several host threads must not
-// overlap.
+// The host-buffer form moves its bytes one of two ways.  Mapped: when the
+// device can address both host buffers (pinned memory), one kernel reads the
+// sizes in place and its last block stores the totals into the host result;
+// no copy-engine transfer, no clearing step.  Copy: one CUDA graph (sizes
+// in, counters cleared, the loop, results out), built on the first call and
+// kept while the arguments stay the same: one launch per call instead of
+// four.  The cached graph and the mapped form's totals are one per process
+// and device: calls from several host threads must not overlap.
 struct HostLoopGraph {
   int dev;
   const uint32_t *h_sizes;
@@ -753,14 +792,40 @@ static int build_host_loop(HostLoopGraph &k) {
   return HA_OK;
 }
 
-extern "C" int ha_throughput_host_c(const uint32_t *h_sizes, uint32_t *d_sizes,
-                                    uint32_t nbytes, uint32_t nthreads, uint32_t block,
-                                    uint32_t nallocs, uint32_t niters, uint64_t *d_out,
-                                    uint64_t *h_out, void *stream) {
-  if (!d_out || !h_out || (h_sizes && !d_sizes) || block == 0 || block > 1024 ||
-      nallocs == 0 || nallocs > kMaxAllocsPerThread)
+// Device view of a host buffer, or nullptr when the device cannot address it
+// (pageable memory).  Asked on every call: a cached answer would outlive a
+// buffer freed and replaced by pageable memory at the same address.
+static const void *mapped_view(const void *h) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
+extern "C" int ha_throughput_host_ex_c(const uint32_t *h_sizes, uint32_t *d_sizes,
+                                       uint32_t nbytes, uint32_t nthreads, uint32_t block,
+                                       uint32_t nallocs, uint32_t niters, uint64_t *d_out,
+                                       uint64_t *h_out, uint32_t transfer, void *stream) {
+  if (!d_out || !h_out || block == 0 || block > 1024 || nallocs == 0 ||
+      nallocs > kMaxAllocsPerThread || transfer > HA_XFER_MAPPED)
     return HA_EINVAL;
   if (nthreads == 0 || niters == 0) return HA_OK;
+  cudaStream_t s = as_stream(stream);
+  if (transfer != HA_XFER_COPY) {
+    auto *mo = static_cast<unsigned long long *>(const_cast<void *>(mapped_view(h_out)));
+    const auto *ms = h_sizes ? static_cast<const uint32_t *>(mapped_view(h_sizes)) : nullptr;
+    if (mo && (!h_sizes || ms)) {
+      ha_throughput_mapped_k<<<blocks_for(nthreads, block), block, 0, s>>>(
+          ms, nbytes, nthreads, nallocs, niters, reinterpret_cast<unsigned long long *>(d_out),
+          mo);
+      if (launch_status() != HA_OK || cudaStreamSynchronize(s) != cudaSuccess) return HA_ECUDA;
+      return HA_OK;
+    }
+    if (transfer == HA_XFER_MAPPED) return HA_EINVAL;
+  }
+  if (h_sizes && !d_sizes) return HA_EINVAL;
   HostLoopGraph want = {};
   if (cudaGetDevice(&want.dev) != cudaSuccess) return HA_ECUDA;
   want.h_sizes = h_sizes;
@@ -781,11 +846,18 @@ extern "C" int ha_throughput_host_c(const uint32_t *h_sizes, uint32_t *d_sizes,
     if (build_host_loop(want) != HA_OK) return HA_ECUDA;
     g_host_loop = want;
   }
-  cudaStream_t s = as_stream(stream);
   if (cudaGraphLaunch(g_host_loop.exec, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return HA_ECUDA;
   return HA_OK;
+}
+
+extern "C" int ha_throughput_host_c(const uint32_t *h_sizes, uint32_t *d_sizes,
+                                    uint32_t nbytes, uint32_t nthreads, uint32_t block,
+                                    uint32_t nallocs, uint32_t niters, uint64_t *d_out,
+                                    uint64_t *h_out, void *stream) {
+  return ha_throughput_host_ex_c(h_sizes, d_sizes, nbytes, nthreads, block, nallocs, niters,
+                                 d_out, h_out, HA_XFER_AUTO, stream);
 }
 
 extern "C" int ha_phase_round_c(int kind, uint32_t nthreads, uint32_t nslots, uint32_t seed,

@@ -189,16 +189,35 @@ int ha_throughput_c(const uint32_t *sizes, uint32_t nbytes, uint32_t nthreads,
                     uint32_t block, uint32_t nallocs, uint32_t niters,
                     uint64_t *out, void *stream);
 
-/* The same loop end to end from host memory: copies h_sizes (nthreads
-   words; NULL for a fixed nbytes) into d_sizes, clears d_out, runs the
-   loop, copies d_out (2 words) to h_out and synchronises the stream.  The
-   four steps run as one CUDA graph, built on the first call and reused
-   while the arguments stay the same (one graph per process: calls from
-   several host threads must not overlap). */
+/* The same loop end to end from host memory: h_sizes (nthreads words;
+   NULL for a fixed nbytes) in, the loop, the two totals out to h_out and to
+   d_out, the stream synchronised.  ha_throughput_host_ex_c with
+   HA_XFER_AUTO.  No counterpart in halloc, whose tests start from device
+   buffers. */
 int ha_throughput_host_c(const uint32_t *h_sizes, uint32_t *d_sizes,
                          uint32_t nbytes, uint32_t nthreads, uint32_t block,
                          uint32_t nallocs, uint32_t niters, uint64_t *d_out,
                          uint64_t *h_out, void *stream);
+
+#define HA_XFER_AUTO 0u   /* mapped when the device can address both host
+                             buffers (pinned memory), else copy */
+#define HA_XFER_COPY 1u   /* copy engine: h_sizes -> d_sizes, d_out cleared,
+                             the loop, d_out -> h_out, as one CUDA graph built
+                             on the first call and reused while the arguments
+                             stay the same */
+#define HA_XFER_MAPPED 2u /* one kernel reads h_sizes in place over the bus
+                             and its last block stores the totals into h_out;
+                             d_sizes is not used.  HA_EINVAL when a buffer
+                             is not device-addressable */
+
+/* ha_throughput_host_c with the transfer chosen (HA_XFER_*).  The cached
+   graph and the mapped form's device totals are one per process and
+   device: calls from several host threads must not overlap.  No counterpart
+   in halloc. */
+int ha_throughput_host_ex_c(const uint32_t *h_sizes, uint32_t *d_sizes,
+                            uint32_t nbytes, uint32_t nthreads, uint32_t block,
+                            uint32_t nallocs, uint32_t niters, uint64_t *d_out,
+                            uint64_t *h_out, uint32_t transfer, void *stream);
 
 /* The same loop with CUDA's in-kernel malloc/free instead of
    hamalloc/hafree: the comparator of the reference's benchmarks

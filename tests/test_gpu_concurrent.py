@@ -182,6 +182,51 @@ def test_throughput_loop_mixed_sizes_host_api(torch_cuda):
         assert H.stats()["used_chunks"] == 0
 
 
+@pytest.mark.parametrize("transfer", [0, 1, 2])
+def test_throughput_loop_host_api_pinned_transfers(torch_cuda, transfer):
+    """Pinned host buffers: the automatic choice (mapped), the copy engine and
+    the mapped form give the same totals, in h_out and in d_out, call after
+    call (the mapped form's device totals start from zero each launch)."""
+    torch = torch_cuda
+    n = 40000  # not a multiple of the block
+    rng = np.random.default_rng(11)
+    sizes = rng.choice(SMALL + [512, 3072], n).astype(np.int32)
+    with allocator(memory=1 << 30) as H:
+        h_sizes = torch.from_numpy(sizes).pin_memory()
+        h_out = torch.zeros(2, dtype=torch.int64).pin_memory()
+        d_sizes = torch.zeros(n, dtype=torch.int32, device="cuda")
+        d_out = torch.zeros(2, dtype=torch.int64, device="cuda")
+        for niters in (3, 3, 1):
+            h_out.zero_()
+            H.throughput_host(h_out.data_ptr(), d_out, n, nallocs=2, niters=niters,
+                              h_sizes=h_sizes.data_ptr(), d_sizes=d_sizes, transfer=transfer)
+            want = plain_checksum(n, 2 * niters)
+            assert h_out.tolist() == [want, 0]
+            assert d_out.cpu().tolist() == [want, 0]
+        # a fixed size, no sizes buffer at all
+        H.throughput_host(h_out.data_ptr(), d_out, n, nbytes=48, niters=2, transfer=transfer)
+        assert h_out.tolist() == [plain_checksum(n, 2), 0]
+        assert H.stats()["used_chunks"] == 0 and H.status() == 0
+
+
+def test_throughput_loop_mapped_needs_pinned_buffers(torch_cuda):
+    """The mapped form refuses pageable host buffers before any launch."""
+    torch = torch_cuda
+    import halloc_b200 as H
+    n = 1024
+    with allocator(memory=512 << 20):
+        d_sizes = torch.zeros(n, dtype=torch.int32, device="cuda")
+        d_out = torch.zeros(2, dtype=torch.int64, device="cuda")
+        h_out = np.zeros(2, np.uint64)
+        h_sizes = np.full(n, 16, np.uint32)
+        with pytest.raises(H.HallocError):
+            H.throughput_host(h_out, d_out, n, h_sizes=h_sizes, d_sizes=d_sizes,
+                              transfer=H.XFER_MAPPED)
+        # the automatic choice falls back to the copy engine for them
+        H.throughput_host(h_out, d_out, n, h_sizes=h_sizes, d_sizes=d_sizes)
+        assert int(h_out[0]) == plain_checksum(n, 1) and int(h_out[1]) == 0
+
+
 def test_cuda_malloc_comparator_checksum(torch_cuda):
     torch = torch_cuda
     n = 4096
