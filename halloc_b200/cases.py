@@ -1,9 +1,9 @@
 """Small instances of the workload kernels, each launched once, for
 profiling one kernel at a time and as short usage examples:
 
-    python -m halloc_b200.cases phase_ref|batched|graph|samples|storm|serve|all
+    python -m halloc_b200.cases phase_ref|phase|batched|graph|samples|storm|serve|all
 
-Every case holds at most a few hundred MB on the device and checks its
+Every case holds at most about 1.1 GB on the device and checks its
 result the way the tests do (counts, checksums, an empty pool at the end);
 a failed check raises.
 """
@@ -46,6 +46,28 @@ def phase_ref(torch) -> None:
     if r["failed"] or r["mallocs"] != r["frees"]:
         raise RuntimeError(f"phase_ref: {r}")
     _done("phase_ref")
+
+
+def phase(torch) -> None:
+    """The mixed-size phase workload, two periods: 1,048,576 threads x 4
+    slots, 1 GiB pool, 16..256 B, allocation rounds (p=0.95) until 91 % of
+    the slots are filled, a free round; then the rest freed: ha_phase_alloc_k,
+    ha_phase_free_k."""
+    n, nslots = 1 << 20, 4
+    sizes = [16, 24, 32, 48, 64, 96, 128, 192, 256]
+    thr = int(0.95 * 2**32)
+    H.init(H.HallocOpts(memory=1 << 30))
+    size_set = torch.tensor(sizes, dtype=torch.int32, device="cuda")
+    slots = torch.zeros(nslots * n, dtype=torch.int64, device="cuda")
+    slot_sz = torch.zeros(nslots * n, dtype=torch.int32, device="cuda")
+    acc = torch.zeros(6, dtype=torch.int64, device="cuda")
+    r = H.phase_run(n, nslots, 0x5EED, 2, thr, thr, int(0.91 * nslots * n), size_set,
+                    len(sizes), slots, slot_sz, acc)
+    if r["failed"] or r["written_sum"] != r["read_sum"] or r["mallocs"] != r["frees"]:
+        raise RuntimeError(f"phase: {r}")
+    print(f"phase: {r['mallocs']} pairs in {r['alloc_rounds']} allocation and "
+          f"{r['free_rounds']} free rounds, {r['kernel_ms']:.3f} ms of kernels")
+    _done("phase")
 
 
 def batched(torch) -> None:
@@ -150,8 +172,8 @@ def serve(torch) -> None:
     _done("serve")
 
 
-CASES = {"phase_ref": phase_ref, "batched": batched, "graph": graph, "samples": samples,
-         "storm": storm, "serve": serve}
+CASES = {"phase_ref": phase_ref, "phase": phase, "batched": batched, "graph": graph,
+         "samples": samples, "storm": storm, "serve": serve}
 
 
 def main(argv) -> None:
