@@ -271,10 +271,14 @@ def run_ours(args, rank, world, local_rank):
     h_out = torch.zeros(2, dtype=torch.int64).pin_memory()
     d_out = torch.zeros(2, dtype=torch.int64, device="cuda")
 
+    # the call takes plain addresses, as a C caller would pass them
+    h_out_p, h_sizes_p = h_out.data_ptr(), h_sizes.data_ptr()
+    d_out_p, d_sizes_p, stream_p = d_out.data_ptr(), d_sizes.data_ptr(), stream.cuda_stream
+
     def e2e_run(transfer):
         def e2e_step():
-            H.throughput_host(h_out.data_ptr(), d_out, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS,
-                              h_sizes=h_sizes.data_ptr(), d_sizes=d_sizes, stream=stream,
+            H.throughput_host(h_out_p, d_out_p, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS,
+                              h_sizes=h_sizes_p, d_sizes=d_sizes_p, stream=stream_p,
                               transfer=transfer)
 
         for _ in range(args.warmup):
