@@ -202,6 +202,54 @@ __device__ __forceinline__ uint32_t slot_hash(uint32_t seed, uint32_t i, uint32_
   return mix32(((i << 2) | s) ^ (round * 0x9E3779B9u) ^ seed);
 }
 
+// A block's payload: the words base, base+1, ... over its sz bytes (sz a
+// multiple of 8), written with 16-byte stores where the block's address and
+// size allow them (every size but 24 B); returns the sum of the words.
+__device__ __forceinline__ unsigned long long write_pattern(void *p, uint32_t sz,
+                                                            uint32_t base) {
+  unsigned long long sum = 0;
+  if ((((uintptr_t)p | sz) & 15u) == 0) {
+    uint4 *q = reinterpret_cast<uint4 *>(p);
+    for (uint32_t w = 0; w < sz / 16; w++) {
+      const uint32_t a = base + 4 * w;
+      const uint4 v = make_uint4(a, a + 1, a + 2, a + 3);  // 32-bit words, wrapping
+      q[w] = v;
+      sum += (unsigned long long)v.x + v.y + v.z + v.w;
+    }
+  } else {
+    uint2 *q = reinterpret_cast<uint2 *>(p);
+    for (uint32_t w = 0; w < sz / 8; w++) {
+      const uint32_t a = base + 2 * w;
+      const uint2 v = make_uint2(a, a + 1);
+      q[w] = v;
+      sum += (unsigned long long)v.x + v.y;
+    }
+  }
+  return sum;
+}
+
+// The sum of a block's words, read with 16-byte loads where possible and
+// eight loads in flight: the read-back waits on DRAM about once per block.
+__device__ __forceinline__ unsigned long long read_sum(const void *p, uint32_t sz) {
+  unsigned long long sum = 0;
+  if ((((uintptr_t)p | sz) & 15u) == 0) {
+    const uint4 *q = reinterpret_cast<const uint4 *>(p);
+#pragma unroll 8
+    for (uint32_t w = 0; w < sz / 16; w++) {
+      const uint4 v = __ldcg(q + w);
+      sum += (unsigned long long)v.x + v.y + v.z + v.w;
+    }
+  } else {
+    const uint2 *q = reinterpret_cast<const uint2 *>(p);
+#pragma unroll 8
+    for (uint32_t w = 0; w < sz / 8; w++) {
+      const uint2 v = __ldcg(q + w);
+      sum += (unsigned long long)v.x + v.y;
+    }
+  }
+  return sum;
+}
+
 // Phase accumulators: [0] slots filled after the round, [1] failed
 // allocations, [2] sum of words written, [3] sum of words read back,
 // [4] allocations, [5] frees.
@@ -224,13 +272,7 @@ __global__ void ha_phase_alloc_k(uint32_t n, uint32_t nslots, uint32_t seed, uin
           const uint32_t sz = size_set[mix32(h ^ 0xA5A5A5A5u) % nsizes];
           p = hamalloc(sz);
           if (p) {
-            const uint32_t base = mix32(h ^ 0x5EED5EEDu);
-            uint2 *q = reinterpret_cast<uint2 *>(p);
-            for (uint32_t w = 0; w < sz / 8; w++) {
-              const uint32_t a = base + 2 * w, b = base + 2 * w + 1;
-              q[w] = make_uint2(a, b);
-              wsum += (unsigned long long)a + b;
-            }
+            wsum += write_pattern(p, sz, mix32(h ^ 0x5EED5EEDu));
             slots[k] = p;
             slot_sz[k] = sz;
             nmal++;
@@ -259,12 +301,7 @@ __global__ void ha_phase_free_k(uint32_t n, uint32_t nslots, uint32_t seed, uint
       void *p = slots[k];
       if (!p) continue;
       if (thr == 0xffffffffu || slot_hash(seed, i, s, round) < thr) {
-        const uint2 *q = reinterpret_cast<const uint2 *>(p);
-        const uint32_t sz = slot_sz[k];
-        for (uint32_t w = 0; w < sz / 8; w++) {
-          const uint2 v = __ldcg(q + w);
-          rsum += (unsigned long long)v.x + v.y;
-        }
+        rsum += read_sum(p, slot_sz[k]);
         hafree(p);
         slots[k] = nullptr;
         nfree++;
