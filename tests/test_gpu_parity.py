@@ -59,6 +59,15 @@ SMALL = [16, 24, 32, 48, 64, 96, 128, 192, 256]
     (dict(memory=256 << 20),
      dict(n=20000, sizes=[0, 1, 15, 16, 17, 24, 25, 33, 47, 49, 255, 257, 383, 385, 1025,
                           3071, 3072, 3073, 4096], pfree=0.35, seed=105)),
+    # other busy / roomy / sparse thresholds (halloc's test harness uses
+    # .745 / .6 / .0125) on 1 MiB slabs of large blocks: 13 to 56 head changes
+    # per size, slabs moving through the sets and back to the free set
+    (dict(memory=128 << 20, halloc_fraction=0.5, sb_sz_sh=20, busy=0.745, roomy=0.6,
+          sparse=0.0125),
+     dict(n=40000, sizes=[1536, 2048, 3072], pfree=0.45, seed=106, drain=0.7, tail=5000)),
+    (dict(memory=64 << 20, halloc_fraction=0.5, sb_sz_sh=20, busy=0.91, roomy=0.5,
+          sparse=0.0125),
+     dict(n=40000, sizes=[768, 3072], pfree=0.4, seed=107, drain=0.9, tail=6000)),
 ])
 def test_serial_trace_matches_model(torch_cuda, opts, targs):
     ops = make_trace(**targs)

@@ -118,6 +118,14 @@ REF_CASES = [
     # size-class edges: zero bytes, one byte, either side of every unit
     # boundary up to the 3 KiB limit and past it
     (dict(memory=256 << 20), dict(n=20000, sizes=EDGES, pfree=0.35, seed=20)),
+    # other busy / roomy / sparse thresholds on 1 MiB slabs of large blocks
+    # (the same traces run on the device in test_gpu_parity)
+    (dict(memory=128 << 20, halloc_fraction=0.5, sb_sz_sh=20, busy=0.745, roomy=0.6,
+          sparse=0.0125),
+     dict(n=40000, sizes=[1536, 2048, 3072], pfree=0.45, seed=106, drain=0.7, tail=5000)),
+    (dict(memory=64 << 20, halloc_fraction=0.5, sb_sz_sh=20, busy=0.91, roomy=0.5,
+          sparse=0.0125),
+     dict(n=40000, sizes=[768, 3072], pfree=0.4, seed=107, drain=0.9, tail=6000)),
 ]
 
 
