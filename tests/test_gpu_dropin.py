@@ -51,3 +51,27 @@ def test_user_program_links_and_runs(torch_cuda):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("OK"), r.stdout
+
+
+REF_SAMPLES = os.path.join(DROPIN, "_build", "ref")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,expect", [
+    ("grid-points", ["allocation performance", "free performance"]),
+    ("add-strings", ["GPU allocation performance", "GPU concatenation performance",
+                     "GPU freeing performance"]),
+    ("random-graph", ["GPU performance"]),
+])
+def test_reference_sample_runs_unchanged(torch_cuda, name, expect):
+    """halloc's own sample program, its source untouched, compiled against
+    include/halloc.h and linked with libhalloc.a (tests/dropin/Makefile): it
+    runs to the end on this allocator (the samples stop with exit(-1) on any
+    CUDA error) and prints its timings."""
+    exe = os.path.join(REF_SAMPLES, name)
+    if not os.path.exists(exe):
+        pytest.skip("built where the reference tree is present: make -C tests/dropin ref-samples")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    for line in expect:
+        assert line in r.stdout, r.stdout
