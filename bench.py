@@ -344,6 +344,8 @@ def run_ours(args, rank, world, local_rank):
             res["serve"] = run_leg("serve")
         if not args.skip_samples:
             res["samples"] = run_leg("samples")
+        if not args.skip_halloc_programs:
+            res["halloc_programs"] = run_halloc_programs()
     return res
 
 
@@ -407,6 +409,8 @@ def leg_main(args):
         out = run_atomic_probe(torch, H)
     elif args.leg == "samples":
         out = run_samples(torch, H, 5)
+    elif args.leg == "halloc_programs":
+        out = run_halloc_programs()
     else:
         out = run_batched(torch, H, 3, not args.no_tune)
     print("LEG " + json.dumps(out), flush=True)
@@ -579,6 +583,148 @@ def run_phase_ref_latency(torch, H) -> dict:
                        "published_kepler_min_avg_max": pub}
         case["published_source"] = "tst/exp/scaling/" + src
         out["cases"].append(case)
+    return out
+
+
+# ---- halloc's own benchmark programs on this allocator ----------------------
+#
+# tst/perf/{phase-throughput,phase-latency,priv-throughput} compiled from the
+# reference tree unchanged against include/halloc.h + libhalloc.a
+# (tests/dropin/Makefile, target ref-tests), run with the arguments of the
+# experiment scripts that produced halloc's published figures.  Their numbers
+# are the harness's own: host clock around every launch, its pair formula.
+
+HALLOC_BIN = os.path.join(ROOT, "tests", "dropin", "_build", "ref")
+PHASE_COMMON = "-f0.95 -F0.05 -e0.91 -m536870912 -g5"  # tst/exp/scaling/exp-run.pl:10-17
+
+# (name, -n -l -s -S arguments, published private pairs, published spree
+# pairs, source); spree = -i1 -t512, private = -i32 -t16
+# (tst/exp/scaling/exp-run.pl:18-50, tst/exp/speed/exp-run.pl:18-34)
+HALLOC_PHASE_CASES = [
+    ("scaling 16 B x1, 1M threads", "-n1048576 -l1 -s16", 1366.76, 940.35,
+     "tst/exp/scaling/exp-log-thru.csv:47"),
+    ("scaling 16 B x4, 1M threads", "-n1048576 -l4 -s16", 1396.75, 1220.92,
+     "tst/exp/scaling/exp-log-thru.csv:48"),
+    ("scaling 256 B x1, 1M threads", "-n1048576 -l1 -s256", 190.58, 557.76,
+     "tst/exp/scaling/exp-log-thru.csv:49"),
+    ("scaling 16 B x1, 32K threads", "-n32768 -l1 -s16", 1012.49, 347.03,
+     "tst/exp/scaling/exp-log-thru.csv:32"),
+    ("scaling 16 B x4, 32K threads", "-n32768 -l4 -s16", 1218.44, 753.21,
+     "tst/exp/scaling/exp-log-thru.csv:33"),
+    ("scaling 256 B x1, 32K threads", "-n32768 -l1 -s256", 621.78, 312.41,
+     "tst/exp/scaling/exp-log-thru.csv:34"),
+    ("scaling 16 B x1, 1K threads", "-n1024 -l1 -s16", 89.53, 15.43,
+     "tst/exp/scaling/exp-log-thru.csv:17"),
+    ("scaling 16 B x4, 1K threads", "-n1024 -l4 -s16", 118.87, 45.02,
+     "tst/exp/scaling/exp-log-thru.csv:18"),
+    ("scaling 256 B x1, 1K threads", "-n1024 -l1 -s256", 92.89, 15.51,
+     "tst/exp/scaling/exp-log-thru.csv:19"),
+    ("single size 16 B", "-n1048576 -l4 -s16", 1401.70, 1220.15,
+     "tst/exp/speed/exp-log-single.csv:2"),
+    ("single size 256 B", "-n838860 -l1 -s256", 194.92, 251.85,
+     "tst/exp/speed/exp-log-single.csv:10"),
+    ("single size 3072 B", "-n69905 -l1 -s3072", 19.68, 30.02,
+     "tst/exp/speed/exp-log-single.csv:17"),
+    ("mixed 8..256 B", "-n1048576 -l1 -s8 -S256", 927.18, 795.18,
+     "tst/exp/speed/exp-log-combi.csv:4"),
+    ("mixed 8..3072 B", "-n139446 -l1 -s8 -S3072", 64.85, 88.33,
+     "tst/exp/speed/exp-log-combi.csv:5"),
+]
+
+# (name, full arguments, published pairs, source): halloc against CUDA's
+# allocator (tst/exp/halloc-vs-scatter/exp-run.pl:12-86) and slab settings
+# (tst/exp/settings/exp-run.pl:7-37)
+HALLOC_OTHER_CASES = [
+    ("spree 4x16 B, 640K threads, halloc",
+     "-f0.9 -F0.2 -e0.71 -m536870912 -g5 -ahalloc -n655360 -l4 -s16 -i1 -t16", 736.18,
+     "tst/exp/halloc-vs-scatter/exp-log-spree.csv:29"),
+    ("spree 4x16 B, 640K threads, CUDA malloc",
+     "-f0.9 -F0.2 -e0.71 -m536870912 -g5 -acuda -n655360 -l4 -s16 -i1 -t16", 0.19,
+     "tst/exp/halloc-vs-scatter/exp-log-spree.csv:31"),
+    ("private 4x16 B, 640K threads, halloc",
+     "-e0.75 -m536870912 -g5 -ahalloc -n655360 -l4 -s16 -f0.9 -F0.35 -e0.75 -i16 -t8", 990.06,
+     "tst/exp/halloc-vs-scatter/exp-log-priv.csv:29"),
+    ("private 4x16 B, 640K threads, CUDA malloc",
+     "-e0.75 -m536870912 -g5 -acuda -n655360 -l4 -s16 -f0.9 -F0.35 -e0.75 -i16 -t1", 1.09,
+     "tst/exp/halloc-vs-scatter/exp-log-priv.csv:31"),
+    ("settings 4x16 B, 4 MiB slabs, busy 0.745",
+     "-f0.95 -F0.05 -e0.91 -n524288 -m536870912 -g5 -i31 -t31 -b22 -B0.745 -s16 -l4", 1441.52,
+     "tst/exp/settings/exp-log.csv:86"),
+    ("settings 4x16 B, 4 MiB slabs, busy 0.835",
+     "-f0.95 -F0.05 -e0.91 -n524288 -m536870912 -g5 -i31 -t31 -b22 -B0.835 -s16 -l4", 1369.94,
+     "tst/exp/settings/exp-log.csv:104"),
+    ("settings 4x16 B, 4 MiB slabs, busy 0.915",
+     "-f0.95 -F0.05 -e0.91 -n524288 -m536870912 -g5 -i31 -t31 -b22 -B0.915 -s16 -l4", 1287.82,
+     "tst/exp/settings/exp-log.csv:120"),
+    ("settings 1x256 B, 2 MiB slabs, busy 0.835",
+     "-f0.95 -F0.05 -e0.91 -n524288 -m536870912 -g5 -i31 -t31 -b21 -B0.835 -s256 -l1", 140.04,
+     "tst/exp/settings/exp-log.csv:63"),
+    ("settings 1x256 B, 4 MiB slabs, busy 0.835",
+     "-f0.95 -F0.05 -e0.91 -n524288 -m536870912 -g5 -i31 -t31 -b22 -B0.835 -s256 -l1", 319.74,
+     "tst/exp/settings/exp-log.csv:105"),
+    ("settings 1x256 B, 8 MiB slabs, busy 0.835",
+     "-f0.95 -F0.05 -e0.91 -n524288 -m536870912 -g5 -i31 -t31 -b23 -B0.835 -s256 -l1", 814.79,
+     "tst/exp/settings/exp-log.csv:147"),
+]
+
+
+def _halloc_program(prog: str, args: str, timeout: int = 300) -> dict:
+    """Runs one of halloc's programs on GPU 0 and parses what it prints."""
+    import re
+    try:
+        p = subprocess.run([os.path.join(HALLOC_BIN, prog), "-D0"] + args.split(),
+                           capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"error": "timed out"}
+    out = {}
+    for line in p.stdout.splitlines():
+        m = re.match(r"(malloc|free|pair) throughput ([0-9.]+)", line)
+        if m:
+            out[m.group(1) + "_mops"] = float(m.group(2))
+        m = re.match(r"(min|avg|max) (malloc|free) latency ([0-9.]+) cycles", line)
+        if m:
+            out.setdefault(m.group(2) + "_cycles", {})[m.group(1)] = float(m.group(3))
+    if p.returncode != 0:
+        out["error"] = (p.stderr or p.stdout)[-300:]
+    return out
+
+
+def run_halloc_programs() -> dict:
+    """halloc's published experiments re-run by halloc's own programs, on
+    this allocator, beside the published (Kepler) figures."""
+    if not os.path.exists(os.path.join(HALLOC_BIN, "phase-throughput")):
+        return {"skipped": "halloc's programs are built where the reference tree is present "
+                           "(make -C tests/dropin ref-tests)"}
+    out = {"unit": "M pairs/s (the harness's formula, host clock per launch)",
+           "how": "tst/perf programs from the reference tree, unchanged, compiled against "
+                  "include/halloc.h and linked with libhalloc.a", "cases": []}
+    r = _halloc_program("priv-throughput", "-n32768 -T128 -s16 -l1 -i10 -m536870912")
+    out["plain"] = {"args": "-n32768 -T128 -s16 -l1 -i10 -m536870912", **r}
+    for name, args, pub_priv, pub_spree, src in HALLOC_PHASE_CASES:
+        for form, extra, pub in (("spree", "-i1 -t512", pub_spree),
+                                 ("private", "-i32 -t16", pub_priv)):
+            a = f"{PHASE_COMMON} {args} {extra}"
+            r = _halloc_program("phase-throughput", a)
+            got = r.get("pair_mops")
+            out["cases"].append({"name": f"{name}, {form}", "args": a, **r,
+                                 "published_kepler_pair_mops": pub, "published_source": src,
+                                 "vs_published": got / pub if got else None})
+    for name, args, pub, src in HALLOC_OTHER_CASES:
+        r = _halloc_program("phase-throughput", args)
+        got = r.get("pair_mops")
+        out["cases"].append({"name": name, "args": args, **r,
+                             "published_kepler_pair_mops": pub, "published_source": src,
+                             "vs_published": got / pub if got else None})
+    out["latency"] = []
+    for n, size, published, src in PHASE_LAT_CASES:
+        a = f"{PHASE_COMMON} -n{n} -l1 -s{size} -i16 -t8"
+        r = _halloc_program("phase-latency", a)
+        out["latency"].append({"args": a, **r, "published_kepler_malloc_free_min_avg_max":
+                               published, "published_source": "tst/exp/scaling/" + src})
+    ratios = [c["vs_published"] for c in out["cases"]
+              if c["vs_published"] and "CUDA" not in c["name"]]
+    out["ok"] = all("error" not in c for c in out["cases"]) and "error" not in out["plain"]
+    out["vs_published_min_max"] = [min(ratios), max(ratios)] if ratios else None
     return out
 
 
@@ -1074,6 +1220,7 @@ def main_ours(args):
             "graph": res.get("graph"),
             "serve": res.get("serve"),
             "samples": samples,
+            "halloc_programs": res.get("halloc_programs"),
             "gpu_launches": args.steps,
             "clocks": res["clocks"],
         }
@@ -1131,7 +1278,10 @@ def main():
     p.add_argument("--skip-serve", action="store_true", help="skip the serving leg")
     p.add_argument("--skip-samples", action="store_true",
                    help="skip the grid-points / add-strings sample leg")
-    p.add_argument("--leg", choices=["phase", "batched", "graph", "serve", "atomics", "samples"],
+    p.add_argument("--skip-halloc-programs", action="store_true",
+                   help="skip halloc's own benchmark programs")
+    p.add_argument("--leg", choices=["phase", "batched", "graph", "serve", "atomics", "samples",
+                                     "halloc_programs"],
                    help=argparse.SUPPRESS)
     p.add_argument("--only-gpu", action="store_true",
                    help="skip the CPU and CUDA-malloc legs (profiling runs)")
