@@ -476,22 +476,39 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
   uint32_t *head = &g_st.head[hs];
   uint32_t *hlock = &g_st.head_lock[hs * kTicketStride];
   cuda::atomic_ref<uint32_t, cuda::thread_scope_device> cached(g_st.cached[hs]);
-  uint32_t seen = ld_relaxed(head);
+  const uint32_t busy = load_class(sid).busy;
+  // One round trip for the head, the memo below and the lock word (test
+  // before test-and-set: while the lock is held, waiting warps only read).
+  const uint32_t seen = ld_relaxed(head);
+  const uint32_t epoch = ld_relaxed(&g_st.set_epoch);
+  const uint32_t memo = ld_relaxed(&g_st.no_slab[hs]);
+  const uint32_t held = ld_relaxed(hlock);
   // A failed search leaves every set it looked at empty, so until a slab is
   // filed somewhere (set_epoch moves) another search would fail the same
   // way: answer at once instead of queueing for the lock to search again.
-  const uint32_t epoch = ld_relaxed(&g_st.set_epoch);
-  if (ld_relaxed(&g_st.no_slab[hs]) == epoch + 1u &&
-      (seen == kNone || used_of(seen) >= load_class(sid).busy))
-    return kNone;
-  // test before test-and-set: while the lock is held, waiting warps only read
-  if (ld_relaxed(hlock) == 0 && try_lock(hlock)) {
-    uint32_t cur = ld_relaxed(head);
-    if (cur != kNone && used_of(cur) < load_class(sid).busy) {
+  if (memo == epoch + 1u && (seen == kNone || used_of(seen) >= busy)) return kNone;
+  if (held == 0 && try_lock(hlock)) {
+    // Under the lock, one round trip again: the head as it is now, the count
+    // of the head seen before (nearly always still the head), and the
+    // prefetched slab, taken on the expectation that the head is replaced.
+    // The exchange comes last so that its acquire does not hold up the loads.
+    const uint32_t cur = ld_relaxed(head);
+    const uint32_t n_seen = seen != kNone ? used_of(seen) : 0u;
+    uint32_t next = cached.exchange(kNone, cuda::memory_order_acquire);
+    if (cur != kNone && (cur == seen ? n_seen : used_of(cur)) < busy) {
+      // not busy after all (the reference's re-check): hand the slab back
+      if (next != kNone) {
+        uint32_t expect = kNone;
+        if (!cached.compare_exchange_strong(expect, next, cuda::memory_order_acq_rel)) {
+          if (lock(&g_st.sb_lock[next])) {
+            detach(next);
+            unlock(&g_st.sb_lock[next]);
+          }
+        }
+      }
       unlock(hlock);
       return cur;
     }
-    uint32_t next = cached.exchange(kNone, cuda::memory_order_acq_rel);
     if (next == kNone) next = find_slab(sid);
     if (next == kNone) {
       st_relaxed(&g_st.no_slab[hs], epoch + 1u);
