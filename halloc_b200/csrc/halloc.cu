@@ -103,6 +103,24 @@ HostDev g_dev[kMaxDevices];
 uint32_t g_hash_scale_pct = 100;
 // head slabs per size for the next init (1 = the reference policy)
 uint32_t g_nheads = 1;
+bool g_nheads_set = false;  // ha_set_heads_c was called
+
+// Head slabs per size for an init.  A program written against halloc.h alone
+// cannot call ha_set_heads_c; HALLOC_HEADS in its environment (a power of
+// two up to kMaxHeads) sets the same knob.  An ha_set_heads_c call wins.
+uint32_t heads_for_init() {
+  if (g_nheads_set) return g_nheads;
+  const char *e = getenv("HALLOC_HEADS");
+  if (!e || !*e) return g_nheads;
+  char *end = nullptr;
+  const unsigned long v = strtoul(e, &end, 10);
+  if (*end || v == 0 || v > ha::kMaxHeads || (v & (v - 1))) {
+    fprintf(stderr, "halloc-b200: HALLOC_HEADS=%s ignored (a power of two from 1 to %u)\n", e,
+            (unsigned)ha::kMaxHeads);
+    return g_nheads;
+  }
+  return (uint32_t)v;
+}
 // bytes backed at the next init, 0 = the whole pool (no growth)
 uint64_t g_growth_initial = 0;
 
@@ -441,7 +459,7 @@ int init_impl(const ha_opts_c &o) {
     cfg.nib_words_sh = sb_sh - 7;
     cfg.set_words = (uint32_t)((nsbs + 31) / 32);
     cfg.sum_words = (cfg.set_words + 31) / 32;
-    cfg.nheads = g_nheads;
+    cfg.nheads = heads_for_init();
     cfg.growth = grow.growth ? 1 : 0;
     if (cudaMemset(meta, 0, meta_bytes) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_cls, cls, sizeof(cls)) != cudaSuccess ||
@@ -874,6 +892,7 @@ extern "C" int ha_dump_state_c(const ha_state_dump_t *d) {
 extern "C" int ha_set_heads_c(uint32_t nheads) {
   if (nheads == 0 || nheads > ha::kMaxHeads || (nheads & (nheads - 1))) return HA_EINVAL;
   g_nheads = nheads;
+  g_nheads_set = true;
   return HA_OK;
 }
 

@@ -153,7 +153,9 @@ int ha_set_hash_scale_c(uint32_t percent);
    head replacement, which spreads the hottest words and the replacement
    work over several slabs.  1 (the default) is the reference policy (its
    compile-time NHEADS, halloc src/slab.h:43) and the only setting whose
-   addresses match it. */
+   addresses match it.  A program that uses only halloc.h sets the same knob
+   with HALLOC_HEADS=<n> in its environment, read at init; a call here wins
+   over the environment. */
 int ha_set_heads_c(uint32_t nheads);
 
 /* Test hook for failure detection: sets the head-replacement lock of size

@@ -340,3 +340,43 @@ def test_kernels_on_concurrent_streams(torch_cuda):
             torch.cuda.synchronize()
             assert_empty(H)
         assert H.status() == 0
+
+
+_HEADS_PROBE = """
+import sys
+sys.path.insert(0, {root!r})
+import torch
+import halloc_b200 as H
+torch.cuda.set_device(0)
+H.init(H.HallocOpts(memory=512 << 20))
+out = torch.zeros(2, dtype=torch.int64, device="cuda")
+H.throughput(out, 1 << 18, nbytes=16, block=128, nallocs=4, niters=2)
+torch.cuda.synchronize()
+st = H.stats()
+assert int(out[1]) == 0 and st["used_chunks"] == 0 and H.status() == 0
+print("head_slabs", st["head_slabs"])
+H.shutdown()
+"""
+
+
+@pytest.mark.parametrize("env,many", [(None, False), ("4", True), ("3", False)])
+def test_heads_from_environment(torch_cuda, env, many):
+    """HALLOC_HEADS reaches programs that only use halloc.h: with 4 head slabs
+    per size a 16-B workload spread over every SM flags more than the one head
+    and one prefetched slab of the reference policy; an invalid value is
+    reported and ignored."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    e = dict(os.environ)
+    e.pop("HALLOC_HEADS", None)
+    if env is not None:
+        e["HALLOC_HEADS"] = env
+    r = subprocess.run([sys.executable, "-c", _HEADS_PROBE.format(root=root)], env=e,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    n = int(r.stdout.split("head_slabs")[1])
+    assert (n > 2) if many else (n <= 2), n
+    if env == "3":
+        assert "HALLOC_HEADS=3 ignored" in r.stderr
