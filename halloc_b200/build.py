@@ -83,7 +83,21 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         _run([cc] + ARCH + ["-shared", "-Xcompiler", "-fPIC"] + objs + [dlink, "-o", SO,
                                                                          "-lcudadevrt"],
              verbose)
+    _build_pyfast(verbose)
     return SO
+
+
+def _build_pyfast(verbose: bool) -> None:
+    """The CPython fast path of the host-buffer loop (csrc/ha_pyfast.c), linked
+    against the shared library beside it."""
+    import sysconfig
+    src = os.path.join(CSRC, "ha_pyfast.c")
+    out = os.path.join(PKG, "_pyfast" + sysconfig.get_config_var("EXT_SUFFIX"))
+    if not _stale(out, [src, SO, os.path.join(INCLUDE, "halloc_c.h")]):
+        return
+    _run(["gcc", "-O2", "-shared", "-fPIC", "-Wall", "-I" + sysconfig.get_paths()["include"],
+          "-I" + INCLUDE, src, "-o", out, "-L" + PKG, "-l:" + os.path.basename(SO),
+          "-Wl,-rpath,$ORIGIN"], verbose)
 
 
 if __name__ == "__main__":

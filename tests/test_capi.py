@@ -59,3 +59,20 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(H, "_lib", None)
     with pytest.raises(H.HallocError):
         H.load()
+
+
+def test_pyfast_binding_checks_arguments():
+    """The CPython binding of the host-buffer loop is built beside the
+    library and reaches the same C ABI function as ctypes: the same argument
+    errors, before any CUDA call."""
+    import halloc_b200 as H
+    assert H._pyfast is not None
+    with pytest.raises(TypeError):
+        H._pyfast.throughput_host(0, 0, 16)
+    with pytest.raises(OverflowError):
+        H._pyfast.throughput_host(0, 0, 1 << 32, 1, 128, 1, 1, 0, 0, 0, 0)
+    with pytest.raises(OverflowError):
+        H._pyfast.throughput_host(-1, 0, 16, 1, 128, 1, 1, 0, 0, 0, 0)
+    # d_out NULL: HA_EINVAL from both bindings
+    args = (0, 0, 16, 1, 128, 1, 1, 0, 8, 0, 0)
+    assert H._pyfast.throughput_host(*args) == H.load().ha_throughput_host_ex_c(*args) == -1
