@@ -97,3 +97,18 @@ def test_corr_test_program(torch_cuda):
     r = _run("test")
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "test PASSED" in r.stdout and "FAILED" not in r.stdout, r.stdout
+
+
+def test_phase_extfrag_program(torch_cuda):
+    """tst/perf/phase-extfrag: halloc's harness calls ha_extfrag(false) and
+    ha_extfrag(true) after every launch of the phase workload; both are
+    fractions of the free slab memory."""
+    r = _run("phase-extfrag", "-f0.95", "-F0.05", "-e0.91", f"-m{MEMORY}", "-g5", "-n1048576",
+             "-l1", "-s8", "-S256", "-i1", "-t8", "-D0")
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    rows = [line.split() for line in r.stdout.splitlines()
+            if line.startswith("external fragmentation")]
+    assert len(rows) == 8, r.stdout
+    for row in rows:
+        real, ideal = float(row[3]), float(row[4])
+        assert 0.0 <= real <= 1.0 and 0.0 <= ideal <= 1.0, row
