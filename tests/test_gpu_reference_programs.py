@@ -112,3 +112,15 @@ def test_phase_extfrag_program(torch_cuda):
     for row in rows:
         real, ideal = float(row[3]), float(row[4])
         assert 0.0 <= real <= 1.0 and 0.0 <= ideal <= 1.0, row
+
+
+@pytest.mark.parametrize("prog,line", [("throughput", "pair throughput"),
+                                       ("latency", "malloc latency")])
+def test_perf_program_runs(torch_cuda, prog, line):
+    """tst/perf/throughput (all mallocs of a launch, then all frees) and
+    tst/perf/latency (clock around each call) with their default options:
+    1 M threads, 4 blocks of 16 B each, 8 tries.  Each checks every pointer
+    for NULL after its malloc launch and stops on one."""
+    r = _run(prog, "-D0", f"-m{MEMORY}")
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert line in r.stdout, r.stdout
