@@ -537,16 +537,22 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
     }
     return next;
   }
+  // Every warp that found the head busy waits here, thousands at once when a
+  // grid storms one size.  Their polls all go to the sectors of the head and
+  // lock words, which the lock holder must write to end the wait, so they
+  // back off to about a microsecond and read the lock word only every
+  // fourth poll (the head word is what normally changes).
   Deadline dl;
   uint32_t pause = 64;
-  for (;;) {
-    if (ld_relaxed(head) != seen || ld_relaxed(hlock) == 0) break;
+  for (uint32_t k = 0;; k++) {
+    if (ld_relaxed(head) != seen) break;
+    if ((k & 3) == 0 && ld_relaxed(hlock) == 0) break;
     if (dl.expired()) {
       raise_status(HA_ST_TIMEOUT);
       return kNone;
     }
     __nanosleep(pause);
-    if (pause < 256) pause *= 2;
+    if (pause < 1024) pause *= 2;
   }
   return ld_relaxed(head);
 }
