@@ -36,7 +36,7 @@ PAIRS_PER_STEP = NTHREADS * NITERS * NALLOCS
 ATOMICS_PER_PAIR = 2  # one bit-array reservation + one release
 # DRAM bytes (read + write) of one launch of the plain kernel, from an ncu
 # capture of the current build (the bench cannot read DRAM counters itself)
-PLAIN_DRAM_BYTES_PER_LAUNCH = 186368
+PLAIN_DRAM_BYTES_PER_LAUNCH = 186624
 METRIC = "16B malloc/free pairs/s"
 WORKLOAD = ("plain: 256 blocks x 128 threads, hamalloc(16) + 16-B write + read-back + hafree, "
             "10 iterations per thread, 512 MiB pool, default halloc_opts_t")
