@@ -1,0 +1,63 @@
+"""Property test of the oracle: random options and random traces, the C
+restatement (oracle/ha_model.c) against halloc's own allocator code built for
+the host (oracle/_ref), op by op and state word by state word.  CPU only.
+
+The options stay where halloc's policy is well defined: the busy threshold
+above the roomy one (with busy at or below roomy a fresh head can already be
+busy, and halloc's head replacement then cycles through the same slabs), and
+pools of at least two slabs."""
+import numpy as np
+import pytest
+from hypothesis import HealthCheck, given, settings
+from hypothesis import strategies as st
+
+import oracle
+from tests.trace_gen import make_trace
+
+needs_ref = pytest.mark.skipif(not oracle.reference_available(),
+                               reason="reference host build (oracle/_ref) absent")
+
+SIZES = [0, 1, 8, 16, 17, 24, 32, 40, 48, 64, 96, 100, 128, 192, 256, 300, 384, 512, 768,
+         1000, 1024, 1536, 2048, 2500, 3072, 3073, 5000]
+
+
+@st.composite
+def options(draw):
+    sb_sz_sh = draw(st.integers(20, 23))
+    slabs = draw(st.integers(2, 80))
+    fraction = draw(st.sampled_from([0.5, 0.75, 1.0]))
+    memory = int(slabs * (1 << sb_sz_sh) / fraction)
+    roomy = draw(st.floats(0.3, 0.7))
+    busy = draw(st.floats(roomy + 0.1, 0.95))
+    sparse = draw(st.floats(0.005, 0.05))
+    return dict(memory=memory, halloc_fraction=fraction, sb_sz_sh=sb_sz_sh, busy=busy,
+                roomy=roomy, sparse=sparse)
+
+
+@st.composite
+def traces(draw):
+    sizes = draw(st.lists(st.sampled_from(SIZES), min_size=1, max_size=6, unique=True))
+    return dict(n=draw(st.integers(1, 4000)), sizes=sizes, pfree=draw(st.floats(0.0, 0.6)),
+                seed=draw(st.integers(0, 2**31 - 1)), drain=draw(st.floats(0.0, 1.0)),
+                tail=draw(st.integers(0, 1000)))
+
+
+def _norm(res):
+    r = np.array(res, np.int64)
+    r[r <= -2] = -2  # large requests: CUDA's allocator, not compared by address
+    return r
+
+
+@needs_ref
+@pytest.mark.timeout(300)
+@settings(max_examples=150, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(opts=options(), targs=traces())
+def test_model_matches_reference_on_random_traces(opts, targs):
+    ops = make_trace(**targs)
+    ref = oracle.Reference(**opts)
+    model = oracle.Model(ref_scan_whole_words=ref.nsbs % 32 != 0, **opts)
+    assert model.nsbs == ref.nsbs
+    rr, mr = _norm(ref.run_ops(ops)), _norm(model.run_ops(ops))
+    diff = np.nonzero(rr != mr)[0]
+    assert len(diff) == 0, f"first difference at op {diff[0]} of {len(ops)}"
+    assert model.state().diff(ref.state()) == []
