@@ -77,3 +77,34 @@ def test_serial_trace_matches_model(torch_cuda, opts, targs):
         res, dump = run_trace(torch_cuda, H, ops)
     assert np.array_equal(res, normalise_large(mres))
     assert m.state().diff(device_state(dump)) == []
+
+
+def test_serial_trace_matches_model_on_random_options(torch_cuda):
+    """Random options and random traces (the strategies of
+    tests/test_oracle_property.py, where the model is pinned to halloc's own
+    code): one device thread gives the model's address for every op and ends
+    in the model's state."""
+    from hypothesis import HealthCheck, given, settings
+
+    from tests.test_oracle_property import options, traces
+
+    @settings(max_examples=60, deadline=None, database=None, derandomize=True,
+              suppress_health_check=[HealthCheck.too_slow, HealthCheck.function_scoped_fixture])
+    @given(opts=options(), targs=traces())
+    def check(opts, targs):
+        ops = make_trace(**targs)
+        m = oracle.Model(**opts)
+        mres = m.run_ops(ops)
+        with allocator(**oracle_opts_to_halloc(opts)) as H:
+            res, dump = run_trace(torch_cuda, H, ops)
+            assert H.status() == 0
+        want = normalise_large(mres)
+        # Blocks above 3 KiB come from CUDA's heap, whose size is fixed by the
+        # first init of the process: there they may be NULL (-1) where the
+        # model, which does not model that heap, answers a handle (-2).
+        large = (np.asarray(ops) > 3072) & (want == -2)
+        assert np.array_equal(res[~large], want[~large])
+        assert np.isin(res[large], (-1, -2)).all()
+        assert m.state().diff(device_state(dump)) == []
+
+    check()
