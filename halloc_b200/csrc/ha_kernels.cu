@@ -569,40 +569,49 @@ __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uin
 // loops that must not call cudaMalloc/cudaFree because those calls
 // synchronise the device and stall every other stream.  For them the
 // persistent form below keeps its scratch -- the task table, the per-batch
-// task counts, the queue and completion counters, and a copy of the step
-// offsets -- in one fixed array in device memory instead.  Every GPU that
-// loads this library holds the array (about 1 MiB) until the process exits.
+// task counts, and the queue and completion counters -- in one fixed array
+// in device memory instead.  Every GPU that loads this library holds the
+// array (about 1 MiB) until the process exits.
 
 constexpr uint32_t kNoAllocMaxTasks = 65536;
 constexpr uint32_t kNoAllocMaxBatches = 1024;
 constexpr size_t kNaTasksOff = 0;
 constexpr size_t kNaBtasksOff = kNaTasksOff + sizeof(BatchTask) * kNoAllocMaxTasks;
 constexpr size_t kNaCtlOff = kNaBtasksOff + 4 * 1280;
-constexpr size_t kNaBatchStartOff = kNaCtlOff + 4 * 1280;
-constexpr size_t kNaFreeStartOff = kNaBatchStartOff + 4 * 1280;
-constexpr size_t kNoAllocScratchBytes = kNaFreeStartOff + 4 * 1280;
+constexpr size_t kNoAllocScratchBytes = kNaCtlOff + 4 * 1280;
 static_assert(kNoAllocMaxBatches + 2 <= 1280, "scratch regions hold nbatch + 2 words");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Builds the task table of ha_batched_prepare_c in the scratch array from the
-// step offsets copied there, and clears the queue and completion counters.
-__global__ void ha_noalloc_tasks_k(unsigned char *scratch, uint32_t nbatch, uint32_t items) {
+// The plan's step offsets, passed by value as a kernel parameter (8 KiB, under
+// the 32 KiB parameter limit): the launch copies them, so the caller's host
+// arrays are free again as soon as the call returns.
+struct NoAllocOffsets {
+  uint32_t batch_start[kNoAllocMaxBatches + 1];
+  uint32_t free_start[kNoAllocMaxBatches + 2];
+};
+
+// Builds the task table of ha_batched_prepare_c in the scratch array and
+// clears the queue and completion counters.  The host has checked that the
+// offsets never decrease and that the table has at most kNoAllocMaxTasks
+// entries; indices are 64-bit and the writes stop at the limit regardless.
+__global__ void ha_noalloc_tasks_k(unsigned char *scratch, uint32_t nbatch, uint32_t items,
+                                   const NoAllocOffsets off) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   BatchTask *tasks = reinterpret_cast<BatchTask *>(scratch + kNaTasksOff);
   uint32_t *btasks = reinterpret_cast<uint32_t *>(scratch + kNaBtasksOff);
   unsigned int *ctl = reinterpret_cast<unsigned int *>(scratch + kNaCtlOff);
-  const uint32_t *bs = reinterpret_cast<const uint32_t *>(scratch + kNaBatchStartOff);
-  const uint32_t *fs = reinterpret_cast<const uint32_t *>(scratch + kNaFreeStartOff);
   uint32_t n = 0;
   for (uint32_t st = 0; st <= nbatch; st++) {
-    for (uint32_t k = fs[st]; k < fs[st + 1]; k += items)
-      tasks[n++] = {k, min(k + items, fs[st + 1]), st, 1u};
+    const uint64_t f1 = off.free_start[st + 1];
+    for (uint64_t k = off.free_start[st]; k < f1 && n < kNoAllocMaxTasks; k += items)
+      tasks[n++] = {(uint32_t)k, (uint32_t)(k + items < f1 ? k + items : f1), st, 1u};
     ctl[1 + st] = 0;
     if (st == nbatch) break;
     btasks[st] = 0;
-    for (uint32_t r = bs[st]; r < bs[st + 1]; r += items) {
-      tasks[n++] = {r, min(r + items, bs[st + 1]), st, 0u};
+    const uint64_t b1 = off.batch_start[st + 1];
+    for (uint64_t r = off.batch_start[st]; r < b1 && n < kNoAllocMaxTasks; r += items) {
+      tasks[n++] = {(uint32_t)r, (uint32_t)(r + items < b1 ? r + items : b1), st, 0u};
       btasks[st]++;
     }
   }
@@ -1089,9 +1098,33 @@ extern "C" int ha_phase_ref_run_c(uint32_t nthreads, uint32_t nallocs, uint32_t 
   return rc;
 }
 
+namespace {
+// Checks a plan's step offsets before anything is launched: batch and free
+// offsets never decrease and end within nreq.  With task_items != 0 it also
+// counts the tasks the persistent form makes of the plan (64-bit, so no
+// offset or task size can wrap it).  HA_EINVAL for a malformed plan.
+int check_plan_offsets(const ha_batch_plan_t *plan, uint32_t task_items, uint64_t *ntasks) {
+  const uint32_t *bs = plan->h_batch_start, *fs = plan->h_free_start;
+  for (uint32_t b = 0; b < plan->nbatch; b++)
+    if (bs[b + 1] < bs[b]) return HA_EINVAL;
+  for (uint32_t st = 0; st <= plan->nbatch; st++)
+    if (fs[st + 1] < fs[st]) return HA_EINVAL;
+  if (bs[plan->nbatch] > plan->nreq || fs[plan->nbatch + 1] > plan->nreq) return HA_EINVAL;
+  if (ntasks && task_items) {
+    uint64_t n = 0;
+    for (uint32_t st = 0; st <= plan->nbatch; st++) {
+      n += ((uint64_t)fs[st + 1] - fs[st] + task_items - 1) / task_items;
+      if (st < plan->nbatch) n += ((uint64_t)bs[st + 1] - bs[st] + task_items - 1) / task_items;
+    }
+    *ntasks = n;
+  }
+  return HA_OK;
+}
+}  // namespace
+
 extern "C" int ha_batched_plain_c(const ha_batch_plan_t *plan, uint32_t block, void *stream) {
   if (!plan || !plan->acc || !plan->h_batch_start || !plan->h_free_start || block == 0 ||
-      block > 1024)
+      block > 1024 || check_plan_offsets(plan, 0, nullptr) != HA_OK)
     return HA_EINVAL;
   cudaStream_t s = as_stream(stream);
   unsigned long long *acc = reinterpret_cast<unsigned long long *>(plan->acc);
@@ -1149,21 +1182,21 @@ extern "C" int ha_batched_prepare_c(const ha_batch_plan_t *plan, uint32_t block,
       block == 0 || block > 1024 || block % 32 || task_items == 0)
     return HA_EINVAL;
   *out = nullptr;
+  uint64_t ntasks = 0;
+  if (check_plan_offsets(plan, task_items, &ntasks) != HA_OK || ntasks > 0xffffffffull)
+    return HA_EINVAL;
   // task table: for each step its free chunks, then its allocation chunks
   std::vector<BatchTask> tasks;
   std::vector<uint32_t> btasks(plan->nbatch + 1, 0);
+  tasks.reserve((size_t)ntasks);
   for (uint32_t st = 0; st <= plan->nbatch; st++) {
-    for (uint32_t k = plan->h_free_start[st]; k < plan->h_free_start[st + 1]; k += task_items) {
-      uint32_t e = k + task_items < plan->h_free_start[st + 1] ? k + task_items
-                                                                : plan->h_free_start[st + 1];
-      tasks.push_back({k, e, st, 1u});
-    }
+    const uint64_t f1 = plan->h_free_start[st + 1];
+    for (uint64_t k = plan->h_free_start[st]; k < f1; k += task_items)
+      tasks.push_back({(uint32_t)k, (uint32_t)(k + task_items < f1 ? k + task_items : f1), st, 1u});
     if (st == plan->nbatch) break;
-    for (uint32_t r = plan->h_batch_start[st]; r < plan->h_batch_start[st + 1];
-         r += task_items) {
-      uint32_t e = r + task_items < plan->h_batch_start[st + 1] ? r + task_items
-                                                                : plan->h_batch_start[st + 1];
-      tasks.push_back({r, e, st, 0u});
+    const uint64_t b1 = plan->h_batch_start[st + 1];
+    for (uint64_t r = plan->h_batch_start[st]; r < b1; r += task_items) {
+      tasks.push_back({(uint32_t)r, (uint32_t)(r + task_items < b1 ? r + task_items : b1), st, 0u});
       btasks[st]++;
     }
   }
@@ -1273,14 +1306,11 @@ extern "C" int ha_batched_run_noalloc_c(const ha_batch_plan_t *plan, uint32_t bl
     return HA_EINVAL;
   if (plan->nbatch > kNoAllocMaxBatches) return HA_ERANGE;
   uint64_t ntasks = 0;
-  for (uint32_t st = 0; st <= plan->nbatch; st++) {
-    ntasks += (plan->h_free_start[st + 1] - plan->h_free_start[st] + (uint64_t)task_items - 1) /
-              task_items;
-    if (st < plan->nbatch)
-      ntasks += (plan->h_batch_start[st + 1] - plan->h_batch_start[st] +
-                 (uint64_t)task_items - 1) / task_items;
-  }
+  if (check_plan_offsets(plan, task_items, &ntasks) != HA_OK) return HA_EINVAL;
   if (ntasks > kNoAllocMaxTasks) return HA_ERANGE;
+  NoAllocOffsets off;
+  memcpy(off.batch_start, plan->h_batch_start, (plan->nbatch + 1) * sizeof(uint32_t));
+  memcpy(off.free_start, plan->h_free_start, (plan->nbatch + 2) * sizeof(uint32_t));
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocDevices) return HA_ECUDA;
   if (!g_noalloc_addr[dev]) {
@@ -1303,15 +1333,8 @@ extern "C" int ha_batched_run_noalloc_c(const ha_batch_plan_t *plan, uint32_t bl
       (uint32_t)nsm * (ctas_per_sm && ctas_per_sm < (uint32_t)fit ? ctas_per_sm : fit);
   cudaStream_t s = as_stream(stream);
   unsigned long long *acc = reinterpret_cast<unsigned long long *>(plan->acc);
-  if (cudaMemcpyAsync(scratch + kNaBatchStartOff, plan->h_batch_start,
-                      (plan->nbatch + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s) !=
-          cudaSuccess ||
-      cudaMemcpyAsync(scratch + kNaFreeStartOff, plan->h_free_start,
-                      (plan->nbatch + 2) * sizeof(uint32_t), cudaMemcpyHostToDevice, s) !=
-          cudaSuccess ||
-      cudaMemsetAsync(acc, 0, 8 * sizeof(uint64_t), s) != cudaSuccess)
-    return HA_ECUDA;
-  ha_noalloc_tasks_k<<<1, 1, 0, s>>>(scratch, plan->nbatch, task_items);
+  if (cudaMemsetAsync(acc, 0, 8 * sizeof(uint64_t), s) != cudaSuccess) return HA_ECUDA;
+  ha_noalloc_tasks_k<<<1, 1, 0, s>>>(scratch, plan->nbatch, task_items, off);
   ha_bpersist_k<<<grid, block, 0, s>>>(
       reinterpret_cast<const BatchTask *>(scratch + kNaTasksOff), (uint32_t)ntasks,
       reinterpret_cast<const uint32_t *>(scratch + kNaBtasksOff), plan->req_size,

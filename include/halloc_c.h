@@ -369,7 +369,9 @@ typedef struct ha_batch_plan_t {
   const uint32_t *h_batch_start; /* host, nbatch+1: batch b = requests
                                     [h_batch_start[b], h_batch_start[b+1]) */
   const uint32_t *h_free_start;  /* host, nbatch+2: step s frees
-                                    free_ids[h_free_start[s] .. [s+1]) */
+                                    free_ids[h_free_start[s] .. [s+1]);
+                                    both offset arrays never decrease and
+                                    end within nreq (else HA_EINVAL) */
   uint64_t *acc; /* device, 8 words: [0] failed allocations, [1] id
                     mismatches, [2] sum of freed request ids, [3]
                     allocations, [4] frees, [5] dependency-wait timeouts */
@@ -400,12 +402,16 @@ int ha_batched_release_c(void *handle);
    fixed array of device memory that every GPU loading this library holds
    until exit (about 1 MiB).  Limits: at most 65,536 tasks (ceil of each
    step's frees and of each batch's requests over task_items, summed) and
-   1,024 batches, else HA_ERANGE.  The first call on a device looks up the
-   array's device address, with that device current; make that first call
-   before any stream capture.  Each call rebuilds the table and clears the
-   counters, but all calls share the one array: calls that overlap on the
-   GPU race, so serialise them (one stream, or events).  The caller still
-   provides the plan's buffers and acc.  No counterpart in the reference. */
+   1,024 batches, else HA_ERANGE; offsets that decrease or run past nreq
+   give HA_EINVAL, checked before anything is launched.  The step offsets
+   (h_batch_start, h_free_start) travel as a kernel parameter, so the host
+   arrays may be reused as soon as the call returns.  The first call on a
+   device looks up the array's device address, with that device current;
+   make that first call before any stream capture.  Each call rebuilds the
+   table and clears the counters, but all calls share the one array: calls
+   that overlap on the GPU race, so serialise them (one stream, or events).
+   The caller still provides the plan's buffers and acc.  No counterpart in
+   the reference. */
 int ha_batched_run_noalloc_c(const ha_batch_plan_t *plan, uint32_t block,
                              uint32_t ctas_per_sm, uint32_t task_items,
                              void *stream);

@@ -50,3 +50,29 @@ def test_noalloc_entry_point_rejects_plans_beyond_its_limit(torch_cuda):
         assert runner.run_noalloc(block=256, task_items=4096) == H.HA_OK
         torch.cuda.synchronize()
         runner.verify()
+
+
+def test_noalloc_entry_point_with_one_task_per_step(torch_cuda):
+    """A task size near 2^32 makes each non-empty step one task; the task
+    table is counted in 64 bits on the host and on the device, so both
+    entry points give the same run as with small tasks."""
+    import halloc_b200 as H
+    from halloc_b200.workloads import BatchedRunner, batched_plan
+    torch = torch_cuda
+    plan = batched_plan(seed=7, nbatch=6, max_batch=1 << 12)
+    with allocator(memory=1 << 30, halloc_fraction=0.5):
+        runner = BatchedRunner(plan, torch)
+        h = runner.prepare(block=256, task_items=1024, graph=False)
+        runner.launch(h)
+        torch.cuda.synchronize()
+        want = runner.verify()
+        runner.release()
+        h = runner.prepare(block=256, task_items=0xFFFFFFF0, graph=False)
+        runner.launch(h)
+        torch.cuda.synchronize()
+        assert runner.verify() == want
+        runner.release()
+        assert runner.run_noalloc(block=256, task_items=0xFFFFFFF0) == H.HA_OK
+        torch.cuda.synchronize()
+        assert runner.verify() == want
+        assert H.stats()["used_chunks"] == 0 and H.status() == 0
