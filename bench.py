@@ -12,7 +12,9 @@ malloc/free is timed beside it, and the reference allocator's own code
 
 N > 1 runs under torchrun as independent replicas (one pool per GPU, no
 collective on the data path; "weak" scaling): value = all pairs / max time.
-Rank 0 prints one JSON line.
+Rank 0 prints one JSON line per secondary leg ({"leg": name, "result": ...};
+N = 1 only), then the headline JSON line last, a few KB at most, carrying
+each leg's one-number summary.
 """
 from __future__ import annotations
 
@@ -38,8 +40,8 @@ ATOMICS_PER_PAIR = 2  # one bit-array reservation + one release
 # capture of the current build (the bench cannot read DRAM counters itself)
 PLAIN_DRAM_BYTES_PER_LAUNCH = 186624
 METRIC = "16B malloc/free pairs/s"
-WORKLOAD = ("plain: 256 blocks x 128 threads, hamalloc(16) + 16-B write + read-back + hafree, "
-            "10 iterations per thread, 512 MiB pool, default halloc_opts_t")
+WORKLOAD = ("plain: 256 x 128 threads, 10 x (hamalloc(16), 16-B write, read-back, hafree), "
+            "512 MiB pool, default halloc_opts_t")
 
 
 def plain_checksum(nthreads: int, per_thread: int) -> int:
@@ -255,7 +257,7 @@ def run_ours(args, rank, world, local_rank):
                 flush.zero_()
                 H.throughput(spare, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS, stream=stream)
             torch.cuda.synchronize()
-        note = "timed region + same load untimed to 0.4 s"
+        note = "timed region + the same load, untimed, to 0.4 s"
     clocks.stop()
     clock_summary = clocks.summary(t_begin, time.time(), note)
     step_ms = [e0.elapsed_time(e1) for e0, e1 in evs]
@@ -312,41 +314,40 @@ def run_ours(args, rank, world, local_rank):
         res["peak"] = measure_atomic_peak(torch, H, stream)
         res["hot_word_rate"] = measure_hot_word_rate(torch, H, stream)
         res["lone_warp_us"] = measure_lone_warp(torch, H, stream, flush)
-        # CUDA in-kernel malloc on the same loop
-        cout = torch.zeros(2, dtype=torch.int64, device="cuda")
-        H.cuda_throughput(cout, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS, stream=stream)
-        torch.cuda.synchronize()
-        cout.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        csteps = max(2, min(5, args.steps))
-        ms = 0.0
-        for _ in range(csteps):
-            flush.zero_()
-            e0.record(stream)
-            H.cuda_throughput(cout, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS, stream=stream)
-            e1.record(stream)
-            e1.synchronize()
-            ms += e0.elapsed_time(e1)
-        cnf = int(cout[1])
-        res["cuda_malloc"] = {"value": PAIRS_PER_STEP * csteps / (ms * 1e-3), "steps": csteps,
-                              "failed_allocs": cnf,
-                              "heap_bytes": H.stats()["cuda_heap_bytes"]}
     H.shutdown()
-    # the secondary legs are one-GPU workloads: run them with the N=1 line only
-    if rank == 0 and world == 1 and not args.only_gpu:
-        if not args.skip_phase:
-            res["phase"] = run_leg("phase")
-        if not args.skip_batched:
-            res["batched"] = run_leg("batched")
-        if not args.skip_graph:
-            res["graph"] = run_leg("graph")
-        if not args.skip_serve:
-            res["serve"] = run_leg("serve")
-        if not args.skip_samples:
-            res["samples"] = run_leg("samples")
-        if not args.skip_halloc_programs:
-            res["halloc_programs"] = run_halloc_programs()
     return res
+
+
+def run_cuda_malloc(torch, H, steps: int) -> dict:
+    """CUDA's in-kernel malloc/free on the same loop, in a process of its
+    own whose device heap is the whole pool size before any kernel runs, as
+    halloc's CUDA-malloc wrapper sets it (tst/common/cuda-malloc-wrapper.h:
+    10-12)."""
+    from cuda.bindings import runtime as rt
+    err, = rt.cudaDeviceSetLimit(rt.cudaLimit.cudaLimitMallocHeapSize, POOL)
+    if err != rt.cudaError_t.cudaSuccess:
+        return {"error": f"cudaDeviceSetLimit: {err}"}
+    err, heap = rt.cudaDeviceGetLimit(rt.cudaLimit.cudaLimitMallocHeapSize)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    cout = torch.zeros(2, dtype=torch.int64, device="cuda")
+    for _ in range(3):
+        H.cuda_throughput(cout, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS, stream=stream)
+    torch.cuda.synchronize()
+    cout.zero_()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        e0.record(stream)
+        H.cuda_throughput(cout, NTHREADS, NBYTES, BLOCK, NALLOCS, NITERS, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+    cs, nf = cout.cpu().tolist()
+    return {"value": PAIRS_PER_STEP * steps / (ms * 1e-3), "unit": "pairs/s", "steps": steps,
+            "failed_allocs": nf, "heap_bytes": int(heap),
+            "ok": nf == 0 and cs == plain_checksum(NTHREADS, NITERS * NALLOCS) * steps}
 
 
 def run_atomic_probe(torch, H) -> dict:
@@ -373,11 +374,12 @@ def run_atomic_probe(torch, H) -> dict:
     return {"unit": "G ops/s", "threads": nthreads, "results": out}
 
 
-def run_leg(name: str) -> dict:
+def run_leg(name: str, steps: int = 20) -> dict:
     """A secondary workload in a child process: its own CUDA context, so
     its pool and CUDA-heap sizes are set afresh."""
     try:
-        p = subprocess.run([sys.executable, os.path.abspath(__file__), "--leg", name],
+        p = subprocess.run([sys.executable, os.path.abspath(__file__), "--leg", name,
+                            "--steps", str(steps)],
                            capture_output=True, text=True, timeout=900)
     except subprocess.TimeoutExpired:
         return {"error": "timed out"}
@@ -411,6 +413,8 @@ def leg_main(args):
         out = run_samples(torch, H, 5)
     elif args.leg == "halloc_programs":
         out = run_halloc_programs()
+    elif args.leg == "cuda_malloc":
+        out = run_cuda_malloc(torch, H, max(2, min(5, args.steps)))
     else:
         out = run_batched(torch, H, 3, not args.no_tune)
     print("LEG " + json.dumps(out), flush=True)
@@ -1109,8 +1113,7 @@ def cpu_sample(kind: str, seconds: float) -> dict:
         tot += dt
         pairs += PAIRS_PER_STEP
     return {"value": pairs / tot, "unit": "pairs/s", "cores": cores,
-            "sample": f"{reps} runs of the full workload ({PAIRS_PER_STEP} pairs each) on "
-                      f"{cores} host threads"}
+            "sample": f"{reps} x the full workload ({PAIRS_PER_STEP} pairs) on {cores} threads"}
 
 
 def cpu_add_strings() -> dict | None:
@@ -1164,6 +1167,115 @@ def reference_kind():
     return "reference" if oracle.reference_available() else "port"
 
 
+def _get(d, *path):
+    """d[path[0]][path[1]]... or None where any step is missing."""
+    for k in path:
+        if isinstance(d, dict):
+            d = d.get(k)
+        elif isinstance(d, list) and isinstance(k, int) and -len(d) <= k < len(d):
+            d = d[k]
+        else:
+            return None
+    return d
+
+
+def leg_summary(name: str, out: dict) -> dict:
+    """The one-number summaries of a secondary leg that the headline line
+    carries; the leg's full result is on its own line before it."""
+    if not isinstance(out, dict) or "error" in out:
+        return {"error": str(_get(out, "error"))[:120]}
+    if name == "phase":
+        return {"pairs_per_s": out.get("value"), "ok": out.get("ok"),
+                "tuned_4_heads_pairs_per_s": _get(out, "tuned_4_heads", "value"),
+                "payload_frac_of_hbm": _get(out, "payload", "frac_of_hbm")}
+    if name == "batched":
+        return {"persistent_pairs_per_s": _get(out, "persistent_graph", "value"),
+                "persistent_vs_plain": out.get("speedup"),
+                "small_only_persistent_vs_plain": _get(out, "small_only", "speedup"),
+                "ok": out.get("ok")}
+    if name == "graph":
+        return {"edges_per_s": out.get("value"), "ok": out.get("ok")}
+    if name == "serve":
+        pts = out.get("points") or []
+        top = max(pts, key=lambda q: q.get("lambda", 0)) if pts else {}
+        return {"lambda": top.get("lambda"), "jobs_per_s": top.get("jobs_per_s"),
+                "p50_us": (top.get("p50_ns") or 0) / 1e3, "p99_us": (top.get("p99_ns") or 0) / 1e3,
+                "ok": out.get("ok")}
+    if name == "samples":
+        return {"ok": out.get("ok")}
+    if name == "halloc_programs":
+        cases = out.get("cases") or []
+        return {"rows": len(cases),
+                "rows_ahead_of_published": sum(1 for c in cases
+                                               if (c.get("vs_published") or 0) > 1.0)}
+    return {}
+
+
+def rounded(x, digits: int = 5):
+    """x with every float rounded to `digits` significant digits (keeps the
+    headline line short enough for a log tail)."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}")
+    if isinstance(x, dict):
+        return {k: rounded(v, digits) for k, v in x.items()}
+    if isinstance(x, list):
+        return [rounded(v, digits) for v in x]
+    return x
+
+
+def print_leg(name: str, out) -> None:
+    print(json.dumps({"leg": name, "result": out}), flush=True)
+
+
+def headline(args, world: int, res: dict, cpu, glibc, cuda_malloc, legs: dict) -> dict:
+    """The last line of a run: the contract's keys for the plain workload,
+    floats rounded, the secondary legs as one-number summaries."""
+    value = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["total_s"])
+    e2e = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["e2e_s"])
+    e2e_copy = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["e2e_copy_s"])
+    peak = res["peak"]["per_sector_returning"] * 1e9
+    peak_coalesced = max(res["peak"]["returning"], res["peak"]["fire_and_forget"]) * 1e9
+    achieved = value / world * ATOMICS_PER_PAIR
+    binding = hot_word_bound(res, value / world) or {}
+    cm_value = _get(cuda_malloc, "value")
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["total_s"] * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "threads": NTHREADS, "iters": NITERS,
+                   "block_bytes": NBYTES, "pool_bytes": POOL,
+                   "pairs_per_step": PAIRS_PER_STEP, "parallelism": f"replicas{world}",
+                   "l2": "flushed between steps (256 MiB write)"},
+        "ok": res["ok"],
+        "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": NTHREADS * 4,
+                "d2h_bytes_per_step": 16,
+                "how": "ha_throughput_host_c, wall clock per step: sizes in and result out "
+                       "through pinned host memory (pinned once, before timing)",
+                "copy_engine_value": e2e_copy},
+        "roofline": {"bound": "l2_atomic", "achieved": achieved / 1e9, "peak": peak / 1e9,
+                     "unit": "Gatomic/s", "frac": achieved / peak,
+                     "traffic": PLAIN_DRAM_BYTES_PER_LAUNCH,
+                     "peak_how": "live: returning u32 atomicOr, a 32-B sector per thread",
+                     "frac_vs_coalesced_peak": achieved / peak_coalesced,
+                     "atomics_per_pair": ATOMICS_PER_PAIR,
+                     "lone_warp_floor_us": binding.get("floor_us"),
+                     "frac_of_lone_warp_floor": binding.get("frac")},
+        "cpu_baseline": cpu,
+        "host_malloc_baseline": ({"value": glibc["value"], "unit": "pairs/s",
+                                  "cores": glibc["cores"]} if glibc else None),
+        "cuda_malloc_baseline": ({"value": cm_value, "unit": "pairs/s",
+                                  "heap_bytes": _get(cuda_malloc, "heap_bytes"),
+                                  "ok": _get(cuda_malloc, "ok")} if cuda_malloc else None),
+        "vs_cuda_malloc": value / world / cm_value if cm_value else None,
+        "legs": legs,
+        "gpu_launches": args.steps,
+        "clocks": res["clocks"],
+    }
+    return rounded(line)
+
+
 def main_ours(args):
     rank, world, local_rank = dist_env()
     if world > 1:
@@ -1174,75 +1286,42 @@ def main_ours(args):
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     res = run_ours(args, rank, world, local_rank)
-    if rank == 0:
-        value = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["total_s"])
-        e2e = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["e2e_s"])
-        e2e_copy = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["e2e_copy_s"])
-        if args.only_gpu:
-            print(json.dumps({"metric": METRIC, "value": value, "e2e": e2e, "ok": res["ok"],
-                              "note": "GPU legs only (profiling run)"}), flush=True)
-            return
-        peak = res["peak"]["per_sector_returning"] * 1e9
-        peak_coalesced = max(res["peak"]["returning"], res["peak"]["fire_and_forget"]) * 1e9
-        achieved = value / world * ATOMICS_PER_PAIR
-        kind = reference_kind()
-        cpu = cpu_sample(kind, args.cpu_seconds) if world == 1 else None
-        if cpu:
-            cpu["kind"] = kind
-        glibc = cpu_sample("glibc", min(3.0, args.cpu_seconds)) if world == 1 else None
-        samples = res.get("samples")
-        if samples is not None and world == 1:
-            samples["add_strings_cpu_baseline"] = cpu_add_strings()
-        line = {
-            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": res["total_s"] * 1e3 / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "threads": NTHREADS, "block": BLOCK,
-                       "iters": NITERS, "block_bytes": NBYTES, "pool_bytes": POOL,
-                       "pairs_per_step": PAIRS_PER_STEP, "parallelism": f"replicas{world}",
-                       "l2": "flushed between timed steps (256 MiB write)"},
-            "ok": res["ok"],
-            "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": NTHREADS * 4,
-                    "d2h_bytes_per_step": 16,
-                    "how": "ha_throughput_host_c from pinned host memory, wall clock per call; "
-                           "mapped transfers: the kernel reads the 128 KiB of request sizes "
-                           "from the pinned host buffer and its last block stores the 16-byte "
-                           "result into the pinned host result",
-                    "copy_engine": {"value": e2e_copy, "unit": "pairs/s",
-                                    "how": "the same call with HA_XFER_COPY: memcpy H2D, "
-                                           "memset, kernel, memcpy D2H as one CUDA graph"}},
-            "roofline": {"bound": "l2_atomic", "achieved": achieved / 1e9, "peak": peak / 1e9,
-                         "unit": "Gatomic/s", "frac": achieved / peak,
-                         "traffic": PLAIN_DRAM_BYTES_PER_LAUNCH,
-                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of "
-                                           "one ncu capture of ha_throughput_k (bytes per "
-                                           "launch; profiles/ha_throughput_k_plain.md)",
-                         "peak_source": "measured live: returning u32 atomicOr, every thread "
-                                        "on its own 32-byte sector (as the hashed bit-array "
-                                        f"probes land): {res['peak']}",
-                         "frac_vs_coalesced_peak": achieved / peak_coalesced,
-                         "algorithmic_atomics_per_pair": ATOMICS_PER_PAIR,
-                         "binding": hot_word_bound(res, value / world)},
-            "cpu_baseline": cpu,
-            "host_malloc_baseline": glibc,
-            "cuda_malloc_baseline": res.get("cuda_malloc"),
-            "vs_cuda_malloc": value / world / res["cuda_malloc"]["value"]
-            if res.get("cuda_malloc") else None,
-            "phase": res.get("phase"),
-            "batched": res.get("batched"),
-            "graph": res.get("graph"),
-            "serve": res.get("serve"),
-            "samples": samples,
-            "halloc_programs": res.get("halloc_programs"),
-            "gpu_launches": args.steps,
-            "clocks": res["clocks"],
-        }
-        print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+    if rank != 0:
+        return
+    if args.only_gpu:
+        value = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["total_s"])
+        e2e = replica_throughput(PAIRS_PER_STEP * args.steps, world, res["e2e_s"])
+        print(json.dumps({"metric": METRIC, "value": value, "e2e": e2e, "ok": res["ok"],
+                          "note": "GPU legs only (profiling run)"}), flush=True)
+        return
+    # the comparator and the secondary legs are one-GPU workloads, each in a
+    # process of its own (fresh pool and CUDA-heap sizes): N=1 line only
+    legs = {}
+    cuda_malloc = None
+    if world == 1:
+        cuda_malloc = run_leg("cuda_malloc", args.steps)
+        print_leg("cuda_malloc", cuda_malloc)
+        for name, skip in (("phase", args.skip_phase), ("batched", args.skip_batched),
+                           ("graph", args.skip_graph), ("serve", args.skip_serve),
+                           ("samples", args.skip_samples),
+                           ("halloc_programs", args.skip_halloc_programs)):
+            if skip:
+                continue
+            out = run_halloc_programs() if name == "halloc_programs" else run_leg(name)
+            if name == "samples" and isinstance(out, dict):
+                out["add_strings_cpu_baseline"] = cpu_add_strings()
+            print_leg(name, out)
+            legs[name] = leg_summary(name, out)
+    kind = reference_kind()
+    cpu = cpu_sample(kind, args.cpu_seconds) if world == 1 else None
+    if cpu:
+        cpu["kind"] = kind
+    glibc = cpu_sample("glibc", min(3.0, args.cpu_seconds)) if world == 1 else None
+    line = headline(args, world, res, cpu, glibc, cuda_malloc, legs)
+    print(json.dumps(line), flush=True)
 
 
 def main_reference(args):
@@ -1296,7 +1375,7 @@ def main():
     p.add_argument("--skip-halloc-programs", action="store_true",
                    help="skip halloc's own benchmark programs")
     p.add_argument("--leg", choices=["phase", "batched", "graph", "serve", "atomics", "samples",
-                                     "halloc_programs"],
+                                     "halloc_programs", "cuda_malloc"],
                    help=argparse.SUPPRESS)
     p.add_argument("--only-gpu", action="store_true",
                    help="skip the CPU and CUDA-malloc legs (profiling runs)")

@@ -12,9 +12,9 @@
  * word for word with the reference built for the host and with the CUDA
  * implementation's device state.
  *
- * Pinned by tests/test_oracle_vs_reference.py against the reference's own
- * sources compiled for the host (oracle/_ref), and by the golden traces in
- * tests/golden/ generated from that build.
+ * Pinned by tests/test_oracle.py and tests/test_oracle_property.py against
+ * the reference's own sources compiled for the host (oracle/_ref), and by
+ * the golden traces in tests/golden/ generated from that build.
  */
 #define _GNU_SOURCE
 #include "ha_model.h"

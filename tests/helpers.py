@@ -121,7 +121,22 @@ def check_blocks(ptrs: np.ndarray, sizes: np.ndarray, pool_base: int, pool_bytes
     assert inpool[small].all(), "small block outside the slab pool"
     assert (~inpool[~small]).all(), "large block inside the slab pool"
     assert (p[inpool] % 8 == 0).all(), "misaligned slab block"
+    # blocks of the power-of-two classes (16-B and 256-B chunks) start on
+    # 16-B boundaries; only the 24-B-chunk classes are 8-B aligned
+    cls = class_bytes(s[inpool])
+    pow2 = (cls & (cls - np.uint64(1))) == 0
+    assert (p[inpool][pow2] % 16 == 0).all(), "power-of-two class block not 16-B aligned"
     return {"n": int(nn.sum()), "nnull": int((~nn).sum())}
+
+
+CLASS_BYTES = np.array([16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536,
+                        2048, 3072], np.uint64)
+
+
+def class_bytes(sizes) -> np.ndarray:
+    """Block size of the size class serving each request size (<= 3072 B)."""
+    sizes = np.maximum(np.asarray(sizes, np.uint64), np.uint64(1))
+    return CLASS_BYTES[np.searchsorted(CLASS_BYTES, sizes)]
 
 
 def expected_slab_state(ptrs, sizes, pool_base: int, sb_sz: int, nsbs: int):
