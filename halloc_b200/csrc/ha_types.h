@@ -47,6 +47,18 @@ constexpr uint32_t kMaxRounds = 1u << 16;  // outer-loop bound of one hamalloc
 constexpr uint32_t kMaxHeads = 8;          // head slabs per size (1 = the reference policy)
 constexpr uint32_t kDefaultWaitUs = 1000000;  // 1 s
 
+// head words: slab id in bits 0-27 (all ones = no head), and in the word of
+// head set 0 the surge level in bits 28-29: 2^level head sets are open for
+// the size (level 0 = the reference's single head)
+constexpr uint32_t kSlabField = 0x0fffffffu;
+constexpr uint32_t kLevelShift = 28;
+constexpr uint32_t kMaxLevel = 3;          // 2^3 = kMaxHeads sets
+constexpr uint32_t kRedirect = 0xfffffffeu;  // replace_head: use head set 0
+// surge trigger: warps that queued for one size's head lock during the life
+// of one head of set 0 (a grid of 1,024 warps can never reach it)
+constexpr uint32_t kSurgeUp = 2048;
+constexpr uint32_t kSurgeDown = 256;
+
 // size class, 32 bytes, the field order of halloc src/size-info.h:8-26
 struct alignas(32) Class {
   uint32_t nchunks;    // chunks of this size's chunk size in one slab
@@ -81,6 +93,7 @@ struct Config {
   uint32_t sum_words;     // ceil(set_words / 32)
   uint32_t nheads;        // head slabs per size, a power of two <= kMaxHeads
   uint32_t growth;        // 1: slabs are backed on demand (ha_grow_c)
+  uint32_t surge;         // 1: head sets 1.. open under contention (nheads == 1 only)
 };
 
 // mutable allocator state (global memory, one instance per device)
@@ -100,6 +113,9 @@ struct State {
   // the last head search for (head, size) hs found nothing at that epoch
   alignas(128) uint32_t set_epoch;
   uint32_t no_slab[kMaxHeads * kNSizes];
+  // warps that queued for a size's head lock since the last change of its
+  // set-0 head, capped near kSurgeUp (one 128-B line per size)
+  alignas(128) uint32_t storm[kNSizes * kTicketStride];
   alignas(128) uint32_t ctr[kMaxSlabs * kCtrStride];
   Desc desc[kMaxSlabs];
   uint32_t sb_lock[kMaxSlabs];
