@@ -27,7 +27,8 @@ __all__ = [
     "grid_check", "grid_free", "strings_alloc", "strings_concat", "strings_free",
     "strings_check", "graph_build", "graph_gather", "serve_run",
     "throughput", "throughput_host", "cuda_throughput", "trace",
-    "atomic_peak", "debug_set_head_lock", "set_hash_scale", "set_heads", "set_growth", "grow",
+    "atomic_peak", "debug_set_head_lock", "set_hash_scale", "set_heads", "set_surge",
+    "set_growth", "grow",
     "trim", "ST_GROW", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
 ]
 
@@ -77,7 +78,9 @@ class _CStats(ctypes.Structure):
                 ("n_head_changes", ctypes.c_uint32), ("n_null", ctypes.c_uint32),
                 ("heap_limit_ok", ctypes.c_uint32), ("head", ctypes.c_uint32 * 16),
                 ("cached", ctypes.c_uint32 * 16), ("growth", ctypes.c_uint32),
-                ("committed_slabs", ctypes.c_uint32), ("unit_bytes", ctypes.c_uint64)]
+                ("committed_slabs", ctypes.c_uint32), ("unit_bytes", ctypes.c_uint64),
+                ("surge_level", ctypes.c_uint32 * 16), ("n_surge_changes", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class _CPhaseResult(ctypes.Structure):
@@ -144,6 +147,7 @@ _SIGS = {
     "ha_debug_set_head_lock_c": (_int, [_u32, _u32]),
     "ha_set_hash_scale_c": (_int, [_u32]),
     "ha_set_heads_c": (_int, [_u32]),
+    "ha_set_surge_c": (_int, [ctypes.c_int]),
     "ha_set_growth_c": (_int, [ctypes.c_uint64]),
     "ha_grow_c": (_int, [ctypes.c_uint64, _vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ha_trim_c": (_int, [ctypes.c_uint64, _vp, ctypes.POINTER(ctypes.c_uint64)]),
@@ -250,9 +254,10 @@ def extfrag(ideal: bool = False) -> float:
 def stats() -> dict:
     s = _CStats()
     _check(load().ha_stats_c(ctypes.byref(s)), "ha_stats_c")
-    d = {f: getattr(s, f) for f, _ in _CStats._fields_ if f not in ("head", "cached")}
-    d["head"] = list(s.head)
-    d["cached"] = list(s.cached)
+    arrays = ("head", "cached", "surge_level")
+    d = {f: getattr(s, f) for f, _ in _CStats._fields_ if f not in arrays + ("reserved",)}
+    for f in arrays:
+        d[f] = list(getattr(s, f))
     return d
 
 
@@ -304,6 +309,12 @@ def set_hash_scale(percent: int) -> None:
 def set_heads(nheads: int) -> None:
     """Head slabs per size for the next init (1 = the reference policy)."""
     _check(load().ha_set_heads_c(nheads), "ha_set_heads_c")
+
+
+def set_surge(on) -> None:
+    """Surge head sets for the next init (see ha_set_surge_c): True, False, or
+    None for the environment's choice (HALLOC_SURGE, on by default)."""
+    _check(load().ha_set_surge_c(-1 if on is None else (1 if on else 0)), "ha_set_surge_c")
 
 
 def debug_set_head_lock(size_id: int, held: bool) -> None:

@@ -19,6 +19,9 @@ from .workloads import BatchedRunner
 
 def _time_point(torch, runner: BatchedRunner, opts: HallocOpts, block: int, items: int,
                 hash_pct: int, reps: int, nheads: int = 1) -> float:
+    """Best of `reps` graph replays of the persistent form at one setting,
+    each replay verified; the knobs go back to the reference's values (hash
+    scale 100, one head) afterwards, whatever happens."""
     set_hash_scale(hash_pct)
     set_heads(nheads)
     init(opts)
@@ -46,29 +49,45 @@ def _time_point(torch, runner: BatchedRunner, opts: HallocOpts, block: int, item
         set_heads(1)
 
 
+SLAB_SHIFTS = (21, 22, 23)          # 2, 4, 8 MiB slabs
+BUSY_FRACTIONS = (0.745, 0.835, 0.91)
+BLOCKS = (128, 256, 512)             # threads per persistent block: 4, 8, 16 warps
+HASH_PCTS = (50, 100, 200)
+HEADS = (2, 4)
+
+
 def autotune(torch, runner: BatchedRunner, memory: int, halloc_fraction: float,
-             reps: int = 3, task_items: int = 2048) -> dict:
+             reps: int = 3, task_items: int = 2048, slab_shifts=SLAB_SHIFTS,
+             busy_fractions=BUSY_FRACTIONS, blocks=BLOCKS, hash_pcts=HASH_PCTS, heads=HEADS,
+             time_point=None) -> dict:
+    """Sweeps the settings in three stages (the reference's settings
+    experiment, tst/exp/settings/exp-run.pl:27-44, sweeps slab size x busy
+    fraction the same way) and returns {"best": point, "points": [...]},
+    each point with its milliseconds.  time_point(torch, runner, opts, block,
+    task_items, hash_pct, reps, nheads) -> ms is _time_point unless given.
+    The first stage always runs at block 256 and hash scale 100."""
+    time_point = time_point or _time_point
     points = []
 
     def opts(sh, busy):
         return HallocOpts(memory=memory, halloc_fraction=halloc_fraction, busy_fraction=busy,
                           sparse_fraction=0.012 if busy <= 0.835 else 0.0125, sb_sz_sh=sh)
 
-    for sh, busy in itertools.product((21, 22, 23), (0.745, 0.835, 0.91)):
-        ms = _time_point(torch, runner, opts(sh, busy), 256, task_items, 100, reps)
+    for sh, busy in itertools.product(slab_shifts, busy_fractions):
+        ms = time_point(torch, runner, opts(sh, busy), 256, task_items, 100, reps, 1)
         points.append({"sb_sz_sh": sh, "busy": busy, "block": 256, "hash_pct": 100, "ms": ms})
     best = min(points, key=lambda p: p["ms"])
-    for block, hp in itertools.product((128, 256, 512), (50, 100, 200)):
+    for block, hp in itertools.product(blocks, hash_pcts):
         if block == 256 and hp == 100:
             continue
-        ms = _time_point(torch, runner, opts(best["sb_sz_sh"], best["busy"]), block,
-                         task_items, hp, reps)
+        ms = time_point(torch, runner, opts(best["sb_sz_sh"], best["busy"]), block,
+                        task_items, hp, reps, 1)
         points.append({"sb_sz_sh": best["sb_sz_sh"], "busy": best["busy"], "block": block,
                        "hash_pct": hp, "ms": ms})
     best = min(points, key=lambda p: p["ms"])
-    for nh in (2, 4):
-        ms = _time_point(torch, runner, opts(best["sb_sz_sh"], best["busy"]), best["block"],
-                         task_items, best["hash_pct"], reps, nh)
+    for nh in heads:
+        ms = time_point(torch, runner, opts(best["sb_sz_sh"], best["busy"]), best["block"],
+                        task_items, best["hash_pct"], reps, nh)
         points.append({"sb_sz_sh": best["sb_sz_sh"], "busy": best["busy"],
                        "block": best["block"], "hash_pct": best["hash_pct"], "nheads": nh,
                        "ms": ms})

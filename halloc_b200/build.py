@@ -7,6 +7,8 @@ Outputs (all git-ignored, all travel with the source tree):
   Users compile with ``-rdc=true`` and link it (include/halloc.h).
 * ``halloc_b200/libhalloc_b200.so`` -- the same allocator plus the batch
   kernels, device-linked, exporting the C ABI of include/halloc_c.h.
+* ``halloc_b200/libhalloc_b200_stamps.so`` -- an instrumented copy (latency
+  stamps, -DHA_STAMPS) for halloc_b200/stamps.py only.
 
 Run ``python -m halloc_b200.build`` (or ``__graft_entry__.build()``).
 """
@@ -29,7 +31,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler", "-fPIC",
                   "-I" + INCLUDE, "-I" + CSRC]
 
-HEADERS = [os.path.join(CSRC, f) for f in ("ha_core.cuh", "ha_types.h", "ha_hist.cuh")] + [
+HEADERS = [os.path.join(CSRC, f) for f in ("ha_core.cuh", "ha_types.h", "ha_hist.cuh",
+                                           "ha_stamp.cuh")] + [
     os.path.join(INCLUDE, f) for f in ("halloc.h", "halloc_c.h")]
 # The allocator's device functions are capped at 64 registers: every kernel
 # that calls hamalloc/hafree inherits the callee's register count at device
@@ -62,6 +65,33 @@ def _run(cmd, verbose):
     subprocess.run(cmd, check=True)
 
 
+STAMPS_SO = os.path.join(PKG, "libhalloc_b200_stamps.so")
+STAMPS_BUILD = os.path.join(PKG, "_build_stamps")
+
+
+def build_stamps(verbose: bool = False) -> str:
+    """The instrumented library (-DHA_STAMPS): the allocator and the batch
+    kernels with latency stamps after every dependent round trip of
+    hamalloc / hafree (see csrc/ha_stamp.cuh).  Used only by
+    halloc_b200/stamps.py, never by the product path."""
+    os.makedirs(STAMPS_BUILD, exist_ok=True)
+    cc = nvcc()
+    objs = []
+    for src in ("halloc.cu", "ha_kernels.cu"):
+        s = os.path.join(CSRC, src)
+        o = os.path.join(STAMPS_BUILD, src.replace(".cu", ".o"))
+        if _stale(o, [s, __file__] + HEADERS):
+            _run([cc] + CUFLAGS + SOURCES[src] + ["-DHA_STAMPS", "-c", s, "-o", o], verbose)
+        objs.append(o)
+    dlink = os.path.join(STAMPS_BUILD, "dlink.o")
+    if _stale(STAMPS_SO, objs):
+        _run([cc] + ARCH + ["-Xcompiler", "-fPIC", "-dlink"] + objs + ["-o", dlink], verbose)
+        _run([cc] + ARCH + ["-shared", "-Xcompiler", "-fPIC"] + objs + [dlink, "-o", STAMPS_SO,
+                                                                         "-lcudadevrt"],
+             verbose)
+    return STAMPS_SO
+
+
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     """Compiles what is out of date; returns the path of the shared library."""
     os.makedirs(BUILD, exist_ok=True)
@@ -84,6 +114,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
                                                                          "-lcudadevrt"],
              verbose)
     _build_pyfast(verbose)
+    build_stamps(verbose)
     return SO
 
 

@@ -26,6 +26,7 @@
 #include <stdint.h>
 
 #include "ha_types.h"
+#include "ha_stamp.cuh"
 
 namespace ha {
 
@@ -102,6 +103,63 @@ __device__ __forceinline__ void red_and(uint32_t *p, uint32_t v) {
 __device__ __forceinline__ void fence_acq_rel() {
   asm volatile("fence.acq_rel.gpu;" ::: "memory");
 }
+
+// Slab metadata accesses (bit arrays, size nibbles, slab counters) carry an
+// L2 evict-last cache policy, so that the metadata of the slabs in use stays
+// in L2 while payload streams through it -- for every kernel that calls
+// hamalloc / hafree, not only those launched on a stream with an access-
+// policy window (ha_l2_persist_c).  Build with -DHA_L2_HINTS=0 for plain
+// accesses.  (halloc's analogue: cudaFuncCachePreferL1 and ld.global.ca
+// metadata loads, src/halloc.cu:279, src/utils.h:141-157.)
+#ifndef HA_L2_HINTS
+#define HA_L2_HINTS 1
+#endif
+#if HA_L2_HINTS
+__device__ __forceinline__ uint64_t meta_policy() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint32_t ld_meta(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.L2::cache_hint.u32 %0, [%1], %2;"
+               : "=r"(v) : "l"(p), "l"(meta_policy()));
+  return v;
+}
+__device__ __forceinline__ uint32_t atom_add_meta(uint32_t *p, uint32_t v) {
+  uint32_t o;
+  asm volatile("atom.relaxed.gpu.global.add.L2::cache_hint.u32 %0, [%1], %2, %3;"
+               : "=r"(o) : "l"(p), "r"(v), "l"(meta_policy()));
+  return o;
+}
+__device__ __forceinline__ uint32_t atom_or_meta(uint32_t *p, uint32_t v) {
+  uint32_t o;
+  asm volatile("atom.relaxed.gpu.global.or.L2::cache_hint.b32 %0, [%1], %2, %3;"
+               : "=r"(o) : "l"(p), "r"(v), "l"(meta_policy()));
+  return o;
+}
+__device__ __forceinline__ uint32_t atom_and_meta(uint32_t *p, uint32_t v) {
+  uint32_t o;
+  asm volatile("atom.relaxed.gpu.global.and.L2::cache_hint.b32 %0, [%1], %2, %3;"
+               : "=r"(o) : "l"(p), "r"(v), "l"(meta_policy()));
+  return o;
+}
+__device__ __forceinline__ void red_or_meta(uint32_t *p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.or.L2::cache_hint.b32 [%0], %1, %2;"
+               ::"l"(p), "r"(v), "l"(meta_policy()));
+}
+__device__ __forceinline__ void red_and_meta(uint32_t *p, uint32_t v) {
+  asm volatile("red.relaxed.gpu.global.and.L2::cache_hint.b32 [%0], %1, %2;"
+               ::"l"(p), "r"(v), "l"(meta_policy()));
+}
+#else
+__device__ __forceinline__ uint32_t ld_meta(const uint32_t *p) { return ld_relaxed(p); }
+__device__ __forceinline__ uint32_t atom_add_meta(uint32_t *p, uint32_t v) { return atom_add(p, v); }
+__device__ __forceinline__ uint32_t atom_or_meta(uint32_t *p, uint32_t v) { return atom_or(p, v); }
+__device__ __forceinline__ uint32_t atom_and_meta(uint32_t *p, uint32_t v) { return atom_and(p, v); }
+__device__ __forceinline__ void red_or_meta(uint32_t *p, uint32_t v) { red_or(p, v); }
+__device__ __forceinline__ void red_and_meta(uint32_t *p, uint32_t v) { red_and(p, v); }
+#endif
 
 // ---------------------------------------------------------------------------
 // status, bounded waits, locks
@@ -199,7 +257,7 @@ __device__ __forceinline__ uint32_t chunk_div(uint32_t v, uint32_t enc) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t *ctr_of(uint32_t sb) { return &g_st.ctr[sb * kCtrStride]; }
 __device__ __forceinline__ uint32_t used_of(uint32_t sb) {
-  return ld_relaxed(ctr_of(sb)) >> kCntShift;
+  return ld_meta(ctr_of(sb)) >> kCntShift;
 }
 __device__ __forceinline__ uint32_t *bits_of(uint32_t sb) {
   return c_cfg.bits + ((size_t)sb << c_cfg.bit_words_sh);
@@ -209,6 +267,17 @@ __device__ __forceinline__ uint32_t *nibs_of(uint32_t sb) {
 }
 __device__ __forceinline__ char *slab_ptr(uint32_t sb) {
   return c_cfg.pool + ((size_t)sb << c_cfg.sb_sh);
+}
+
+// head words: the slab (kNone when the field is all ones) and, in head set
+// 0's word of a size, the surge level (head sets 0 .. 2^level - 1 are open)
+__device__ __forceinline__ uint32_t head_slab(uint32_t w) {
+  const uint32_t sb = w & kSlabField;
+  return sb == kSlabField ? kNone : sb;
+}
+__device__ __forceinline__ uint32_t head_level(uint32_t w) { return w >> kLevelShift; }
+__device__ __forceinline__ uint32_t head_word(uint32_t sb, uint32_t level) {
+  return (sb == kNone ? kSlabField : sb) | (level << kLevelShift);
 }
 
 // ---------------------------------------------------------------------------
@@ -375,6 +444,57 @@ __device__ __forceinline__ void make_head(uint32_t sb) {
   red_add(ctr_of(sb), kHeadFlag);
 }
 
+// Stops using a head of a surge set (or its prefetched slab) before it is
+// busy and files it where a later head search finds it.  Unlike detach (the
+// reference's rules for a busy head), a slab between the roomy and busy
+// thresholds goes to the busy set of its size, so no free space is stranded
+// outside every set.  Caller holds the slab lock.
+__device__ __noinline__ void retire(uint32_t sb) {
+  Desc *d = &g_st.desc[sb];
+  st_relaxed(&d->is_head, 0);
+  const uint32_t before = atom_add(ctr_of(sb), 0u - kHeadFlag);
+  const uint32_t n = before >> kCntShift;
+  const uint32_t sid = ld_relaxed(&d->size_id), cid = ld_relaxed(&d->chunk_id);
+  if (sid >= kNSizes || cid >= kNChunkIds) return;
+  if (n == 0) {
+    try_release(sb, cid, true);
+    return;
+  }
+  const Class c = load_class(sid);
+  if (n <= c.sparse)
+    set_put(kSetSparse + cid, sb);
+  else if (n <= c.roomy)
+    set_put(kSetRoomy + sid, sb);
+  else if (n <= c.busy)
+    set_put(kSetBusy + sid, sb);
+}
+
+// Closes surge head set hs (set 1 or above): its head and its prefetched slab
+// are retired.  Unless `force`, only while the size's set-0 head word says
+// the set is closed (a set opened again meanwhile keeps its head).
+__device__ __noinline__ void retire_set(uint32_t hs, bool force) {
+  const uint32_t sid = hs % kNSizes, set = hs / kNSizes;
+  uint32_t *hlock = &g_st.head_lock[hs * kTicketStride];
+  if (!lock(hlock)) return;
+  if (!force && set < (1u << head_level(ld_relaxed(&g_st.head[sid])))) {
+    unlock(hlock);
+    return;
+  }
+  const uint32_t old = head_slab(ld_relaxed(&g_st.head[hs]));
+  st_release(&g_st.head[hs], kSlabField);
+  cuda::atomic_ref<uint32_t, cuda::thread_scope_device> cached(g_st.cached[hs]);
+  const uint32_t pre = cached.exchange(kNone, cuda::memory_order_acq_rel);
+  unlock(hlock);
+  if (old != kNone && lock(&g_st.sb_lock[old])) {
+    retire(old);
+    unlock(&g_st.sb_lock[old]);
+  }
+  if (pre != kNone && lock(&g_st.sb_lock[pre])) {
+    retire(pre);
+    unlock(&g_st.sb_lock[pre]);
+  }
+}
+
 // Picks the next head slab for a size: roomy slabs of the size, sparse slabs
 // of its chunk size, free slabs, then busy slabs at most half way from busy
 // to full (halloc src/slab.cuh:259-372).  kNone if there is none, or if a
@@ -459,64 +579,130 @@ __device__ __noinline__ uint32_t find_slab(uint32_t sid) {
   return kNone;
 }
 
-// Gives size `sid` a new head slab once the current one has reached the busy
-// threshold: the prefetched ("cached") slab first, then a search; the next
-// slab is prefetched right away.  One lane per warp calls this.  A caller
-// that loses the race for the size's lock waits (bounded) until the head
-// changes or the lock is released (halloc src/slab.cuh:378-445).
+// Whether any surge set of size sid holds a head or a prefetched slab (also
+// a set closed by a level change whose retirement lost a race).
+__device__ __noinline__ bool surge_slabs_held(uint32_t sid) {
+  bool any = false;
+  for (uint32_t k = 1; k < kMaxHeads; k++) {
+    const uint32_t hs = k * kNSizes + sid;
+    any |= head_slab(ld_relaxed(&g_st.head[hs])) != kNone;
+    any |= ld_relaxed(&g_st.cached[hs]) != kNone;
+  }
+  return any;
+}
+
+// Hands a slab taken for head slot hs back to hs's prefetch slot, or, when
+// another prefetch landed there first, files it again.
+__device__ __noinline__ void hand_back(uint32_t hs, uint32_t sb) {
+  cuda::atomic_ref<uint32_t, cuda::thread_scope_device> cached(g_st.cached[hs]);
+  uint32_t expect = kNone;
+  if (!cached.compare_exchange_strong(expect, sb, cuda::memory_order_acq_rel)) {
+    if (lock(&g_st.sb_lock[sb])) {
+      detach(sb);
+      unlock(&g_st.sb_lock[sb]);
+    }
+  }
+}
+
+// Gives head slot hs (= set * kNSizes + size id) a new head slab once the
+// current one has reached the busy threshold: the prefetched ("cached") slab
+// first, then a search; the next slab is prefetched right away.  One lane
+// per warp calls this.  A caller that loses the race for the slot's lock
+// waits (bounded) until the head changes or the lock is released (halloc
+// src/slab.cuh:378-445).
 //
 // The lock covers only the switch of the head.  Filing the old head and
 // prefetching the next slab, which the reference also does under the lock,
 // run after it is released, so other warps can use the new head meanwhile;
 // a single thread still performs the reference's steps in the reference's
 // order.  Two prefetches can then overlap: the loser hands its slab back.
+//
+// Surge sets (c_cfg.surge): when thousands of warps queue for one size's
+// head (a grid far larger than its head's free space), the lock holder of
+// set 0 opens more head sets for the size, each serving the SMs whose id
+// modulo 2^level names it, and closes them again as the queue shrinks.  The
+// level travels in set 0's head word.  A set-k slot answers kRedirect (use
+// set 0) when the set is closed or finds no slab; when set 0 itself finds no
+// slab while surge sets are open, it closes them all (their heads are filed
+// by occupancy) and searches again, so NULL still means what it means with
+// one head.  A lone thread never waits for a lock, so it never opens a set
+// and gets exactly the reference's addresses.
 __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
-  // hs = ihead * kNSizes + size id
-  const uint32_t sid = hs % kNSizes;
+  const uint32_t sid = hs % kNSizes, set = hs / kNSizes;
+  const bool surge_set = c_cfg.surge && set != 0;
+  const uint32_t none = surge_set ? kRedirect : kNone;  // "no head" answer
   uint32_t *head = &g_st.head[hs];
   uint32_t *hlock = &g_st.head_lock[hs * kTicketStride];
   cuda::atomic_ref<uint32_t, cuda::thread_scope_device> cached(g_st.cached[hs]);
   const uint32_t busy = load_class(sid).busy;
-  // One round trip for the head, the memo below and the lock word (test
-  // before test-and-set: while the lock is held, waiting warps only read).
-  const uint32_t seen = ld_relaxed(head);
+  // One round trip for the head, the memo below, the lock word and (surge
+  // sets) set 0's head word (test before test-and-set: while the lock is
+  // held, waiting warps only read).
+  const uint32_t wseen = ld_relaxed(head);
   const uint32_t epoch = ld_relaxed(&g_st.set_epoch);
   const uint32_t memo = ld_relaxed(&g_st.no_slab[hs]);
   const uint32_t held = ld_relaxed(hlock);
+  const uint32_t w0 = surge_set ? ld_relaxed(&g_st.head[sid]) : 0u;
+  const uint32_t seen = head_slab(wseen);
+  if (surge_set && set >= (1u << head_level(w0))) return kRedirect;
   // A failed search leaves every set it looked at empty, so until a slab is
   // filed somewhere (set_epoch moves) another search would fail the same
   // way: answer at once instead of queueing for the lock to search again.
-  if (memo == epoch + 1u && (seen == kNone || used_of(seen) >= busy)) return kNone;
+  if (memo == epoch + 1u && (seen == kNone || used_of(seen) >= busy)) return none;
   if (held == 0 && try_lock(hlock)) {
     // Under the lock, one round trip again: the head as it is now, the count
-    // of the head seen before (nearly always still the head), and the
-    // prefetched slab, taken on the expectation that the head is replaced.
-    // The exchange comes last so that its acquire does not hold up the loads.
-    const uint32_t cur = ld_relaxed(head);
+    // of the head seen before (nearly always still the head), set 0's word
+    // (surge sets) and the prefetched slab, taken on the expectation that
+    // the head is replaced.  The exchange comes last so that its acquire
+    // does not hold up the loads.
+    const uint32_t wcur = ld_relaxed(head);
+    const uint32_t cur = head_slab(wcur);
     const uint32_t n_seen = seen != kNone ? used_of(seen) : 0u;
+    const uint32_t w0now = surge_set ? ld_relaxed(&g_st.head[sid]) : 0u;
     uint32_t next = cached.exchange(kNone, cuda::memory_order_acquire);
+    if (surge_set && set >= (1u << head_level(w0now))) {
+      // the set closed while this warp came for its lock
+      unlock(hlock);
+      if (next != kNone && lock(&g_st.sb_lock[next])) {
+        retire(next);
+        unlock(&g_st.sb_lock[next]);
+      }
+      return kRedirect;
+    }
     if (cur != kNone && (cur == seen ? n_seen : used_of(cur)) < busy) {
       // not busy after all (the reference's re-check): hand the slab back
-      if (next != kNone) {
-        uint32_t expect = kNone;
-        if (!cached.compare_exchange_strong(expect, next, cuda::memory_order_acq_rel)) {
-          if (lock(&g_st.sb_lock[next])) {
-            detach(next);
-            unlock(&g_st.sb_lock[next]);
-          }
-        }
-      }
+      if (next != kNone) hand_back(hs, next);
       unlock(hlock);
       return cur;
     }
+    const uint32_t level = set == 0 ? head_level(wcur) : 0u;
+    uint32_t nlevel = level;
     if (next == kNone) next = find_slab(sid);
+    if (next == kNone && set == 0 && c_cfg.surge && surge_slabs_held(sid)) {
+      // short of slabs while surge sets hold heads: close them all, which
+      // files their heads and prefetched slabs where this search finds them
+      for (uint32_t k = 1; k < kMaxHeads; k++) retire_set(k * kNSizes + sid, true);
+      nlevel = 0;
+      next = find_slab(sid);
+    }
     if (next == kNone) {
       st_relaxed(&g_st.no_slab[hs], epoch + 1u);
+      if (nlevel != level) st_release(head, head_word(cur, nlevel));
       unlock(hlock);
-      return kNone;
+      return none;
     }
-    st_release(head, next);
+    if (set == 0 && c_cfg.surge && nlevel == level) {
+      // how many warps queued for this size's heads during the old head's
+      // life: open a level above kSurgeUp, close one below kSurgeDown
+      const uint32_t storm = atomicExch(&g_st.storm[sid * kTicketStride], 0u);
+      if (storm >= kSurgeUp && level < kMaxLevel)
+        nlevel = level + 1;
+      else if (storm < kSurgeDown && level > 0)
+        nlevel = level - 1;
+    }
+    st_release(head, head_word(next, nlevel));
     red_add(&g_st.n_head_changes, 1);
+    if (nlevel != level) red_add(&g_st.n_surge_changes, 1);
     unlock(hlock);
     if (cur != kNone) {
       if (lock(&g_st.sb_lock[cur])) {
@@ -524,28 +710,28 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
         unlock(&g_st.sb_lock[cur]);
       }
     }
+    // a level closed by the storm count: retire the heads of its sets
+    for (uint32_t k = 1u << nlevel; k < (1u << level) && nlevel < level; k++)
+      retire_set(k * kNSizes + sid, false);
     const uint32_t pre = find_slab(sid);
-    if (pre != kNone) {
-      uint32_t expect = kNone;
-      if (!cached.compare_exchange_strong(expect, pre, cuda::memory_order_acq_rel)) {
-        // another replacement prefetched first: file this slab again
-        if (lock(&g_st.sb_lock[pre])) {
-          detach(pre);
-          unlock(&g_st.sb_lock[pre]);
-        }
-      }
-    }
+    if (pre != kNone) hand_back(hs, pre);
     return next;
   }
   // Every warp that found the head busy waits here, thousands at once when a
   // grid storms one size.  Their polls all go to the sectors of the head and
   // lock words, which the lock holder must write to end the wait, so they
   // back off to about a microsecond and read the lock word only every
-  // fourth poll (the head word is what normally changes).
+  // fourth poll (the head word is what normally changes).  With surge sets
+  // on, each waiting warp is counted once (up to the threshold) for the
+  // lock holder's next decision.
+  if (c_cfg.surge) {
+    uint32_t *storm = &g_st.storm[sid * kTicketStride];
+    if (ld_relaxed(storm) < kSurgeUp) red_add(storm, 1u);
+  }
   Deadline dl;
   uint32_t pause = 64;
   for (uint32_t k = 0;; k++) {
-    if (ld_relaxed(head) != seen) break;
+    if (ld_relaxed(head) != wseen) break;
     if ((k & 3) == 0 && ld_relaxed(hlock) == 0) break;
     if (dl.expired()) {
       raise_status(HA_ST_TIMEOUT);
@@ -554,9 +740,9 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
     __nanosleep(pause);
     if (pause < 1024) pause *= 2;
   }
-  return ld_relaxed(head);
+  const uint32_t now = head_slab(ld_relaxed(head));
+  return now == kNone ? none : now;
 }
-
 // ---------------------------------------------------------------------------
 // allocation
 // ---------------------------------------------------------------------------
@@ -618,20 +804,20 @@ __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t
     for (uint32_t i = 1; i < kLookahead; i++)
       pp[i] = next_probe(first, round + i - 1, c.ncib, c.nchunks, mn, c.hash_step, mh);
 #pragma unroll
-    for (uint32_t i = 0; i < kLookahead; i++) ww[i] = ld_relaxed(&bits[pp[i] >> 5]);
+    for (uint32_t i = 0; i < kLookahead; i++) ww[i] = ld_meta(&bits[pp[i] >> 5]);
     const uint32_t count = used_of(sb);
 #pragma unroll
     for (uint32_t i = 0; i < kLookahead; i++) {
       const uint32_t r = round + i;  // try number of position pp[i]
       const uint32_t mask = block << (pp[i] & 31);
       if (!(ww[i] & mask)) {
-        const uint32_t old = atom_or(&bits[pp[i] >> 5], mask);
+        const uint32_t old = atom_or_meta(&bits[pp[i] >> 5], mask);
         if (!(old & mask)) {
           pos = pp[i];
           round = r;
           return true;
         }
-        if (~old & mask) red_and(&bits[pp[i] >> 5], ~mask | (old & mask));
+        if (~old & mask) red_and_meta(&bits[pp[i] >> 5], ~mask | (old & mask));
       }
       // try r failed
       if (r % kCountCheck == kCountCheck - 1 && count >= c.busy) {
@@ -662,7 +848,7 @@ __device__ __forceinline__ bool commit(uint32_t rmask, uint32_t sb, uint32_t nci
   const uint32_t total = __reduce_add_sync(grp, ncib);
   const uint32_t lead = __ffs(grp) - 1;
   uint32_t before = 0;
-  if (lane_id() == lead) before = atom_add(ctr_of(sb), total << kCntShift);
+  if (lane_id() == lead) before = atom_add_meta(ctr_of(sb), total << kCntShift);
   before = __shfl_sync(grp, before, lead);
   const bool ok = ((before >> kChunkShift) & kChunkField) == cid;
   const uint32_t n0 = before >> kCntShift;
@@ -670,7 +856,7 @@ __device__ __forceinline__ bool commit(uint32_t rmask, uint32_t sb, uint32_t nci
   const uint32_t cmask = __ballot_sync(rmask, !ok);
   if (!ok) {
     // the slab changed chunk size under us: give the block back
-    red_and(&bits_of(sb)[pos >> 5], ~(block << (pos & 31)));
+    red_and_meta(&bits_of(sb)[pos >> 5], ~(block << (pos & 31)));
     count_down(cmask, sb, ncib);
   }
   return ok;
@@ -679,7 +865,7 @@ __device__ __forceinline__ bool commit(uint32_t rmask, uint32_t sb, uint32_t nci
 __device__ __forceinline__ void *publish(uint32_t sb, uint32_t pos, uint32_t enc,
                                          uint32_t ncib) {
   const uint32_t off = chunk_mul(pos, enc);
-  red_or(&nibs_of(sb)[off >> 7], ncib << ((off >> 2) & 28));
+  red_or_meta(&nibs_of(sb)[off >> 7], ncib << ((off >> 2) & 28));
   return slab_ptr(sb) + off;
 }
 
@@ -692,12 +878,12 @@ constexpr uint32_t kMidRound = 4;  // continue the current probe call at pos
 // src/slab.cuh:453-535), for the whole warp `warp`: new head slabs for the
 // lanes that need one (one lane per size at a time), then further probe
 // calls for lanes still without a block.  Every lane of `warp` calls it.
-__device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hbase, uint32_t nbytes,
+__device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t nbytes,
                                           uint32_t ticket, uint32_t sb, uint32_t pos,
                                           uint32_t round, uint32_t flags, void *p) {
+  // hs: this lane's head slot (head set * kNSizes + size id)
   const uint32_t me = lane_id();
   const uint32_t sid = size_class(nbytes);
-  const uint32_t hs = hbase + sid;  // this lane's (head, size) slot
   const Class c = load_class(sid);
   const uint4 mm = __ldg(&g_mod[sid]);
   const uint64_t mn = mod_magic(mm.x, mm.y), mh = mod_magic(mm.z, mm.w);
@@ -710,14 +896,21 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hbase, uint32_
     uint32_t nmask = __ballot_sync(warp, need_head);
     while (nmask) {
       const uint32_t lead = __ffs(nmask) - 1;
-      const uint32_t lsid = __shfl_sync(warp, sid, lead);
+      const uint32_t lhs = __shfl_sync(warp, hs, lead);
       uint32_t nsb = 0;
       if (me == lead) nsb = replace_head(hs);
       nsb = __shfl_sync(warp, nsb, lead);
-      if (need_head && sid == lsid) {
-        sb = nsb;
-        need_head = false;
-        if (nsb == kNone) want = false;
+      if (need_head && hs == lhs) {
+        if (nsb == kRedirect) {
+          // the lane's surge set closed or ran dry: go on in head set 0
+          hs = sid;
+          sb = head_slab(ld_relaxed(&g_st.head[hs]));
+          need_head = sb == kNone;
+        } else {
+          sb = nsb;
+          need_head = false;
+          if (nsb == kNone) want = false;
+        }
       }
       nmask = __ballot_sync(warp, need_head);
     }
@@ -760,25 +953,42 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hbase, uint32_
 // else (further probes, head replacement, exhaustion) continues in
 // malloc_slow exactly where the reference's loop would.
 // (halloc src/halloc.cu:125-182)
+// Tickets of head slot hs for the lanes of `mask` that name it: consecutive
+// values in lane order, one atomic per slot and warp.
+__device__ __forceinline__ uint32_t take_ticket(uint32_t mask, uint32_t hs) {
+  const uint32_t grp = __match_any_sync(mask, hs);
+  const uint32_t lead = __ffs(grp) - 1;
+  uint32_t base = 0;
+  if (lane_id() == lead) base = atom_add(&g_st.ticket[hs * kTicketStride], __popc(grp));
+  base = __shfl_sync(grp, base, lead);
+  return base + __popc(grp & lanemask_lt());
+}
+
 __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
   const uint32_t warp = __activemask();
   const uint32_t sid = size_class(nbytes);
   const uint4 ca = __ldg(reinterpret_cast<const uint4 *>(&g_cls[sid]));
   const uint32_t nchunks = ca.x, enc = ca.y, cid = ca.z, ncib = ca.w;
-  // head slab set of this SM (always 0 with the reference's single head)
-  const uint32_t hbase = (sm_id() & (c_cfg.nheads - 1)) * kNSizes;
-  uint32_t sb = ld_relaxed(&g_st.head[hbase + sid]);
-
-  // ticket: consecutive values for lanes of one size, in lane order
-  uint32_t ticket;
+  // head slot: fixed head set of this SM with ha_set_heads_c (set 0 with the
+  // reference's single head); head word and ticket in one round trip
+  const uint32_t smid = sm_id();
+  HA_STAMP(kStMallocIn, smid);
+  uint32_t hs = (smid & (c_cfg.nheads - 1)) * kNSizes + sid;
+  const uint32_t w = ld_relaxed(&g_st.head[hs]);
+  uint32_t ticket = take_ticket(warp, hs);
+  uint32_t sb = head_slab(w);
+  HA_STAMP(kStMallocTicket, ticket ^ w);
   {
-    const uint32_t grp = __match_any_sync(warp, sid);
-    const uint32_t lead = __ffs(grp) - 1;
-    uint32_t base = 0;
-    if (lane_id() == lead)
-      base = atom_add(&g_st.ticket[(hbase + sid) * kTicketStride], __popc(grp));
-    base = __shfl_sync(grp, base, lead);
-    ticket = base + __popc(grp & lanemask_lt());
+    // surge sets open for this size (set 0's word says how many): lanes on
+    // the SMs of set k > 0 take that set's head and ticket instead, one
+    // round trip more, only while the size is under a storm
+    const uint32_t k = smid & ((1u << head_level(w)) - 1u);
+    const uint32_t moved = __ballot_sync(warp, k != 0);
+    if (moved && k != 0) {
+      hs = k * kNSizes + sid;
+      sb = head_slab(ld_relaxed(&g_st.head[hs]));
+      ticket = take_ticket(moved, hs);
+    }
   }
   const uint4 mm = __ldg(&g_mod[sid]);
   const uint64_t mn = mod_magic(mm.x, mm.y);
@@ -792,11 +1002,12 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
   } else {
     const uint32_t mask = block << (pos & 31);
     uint32_t *w = &bits_of(sb)[pos >> 5];
-    const uint32_t old = atom_or(w, mask);
+    const uint32_t old = atom_or_meta(w, mask);
+    HA_STAMP(kStMallocProbe, old);
     if (!(old & mask)) {
       reserved = true;
     } else {
-      if (~old & mask) red_and(w, ~mask | (old & mask));
+      if (~old & mask) red_and_meta(w, ~mask | (old & mask));
       // try 0 failed: no count check at an even try; move to try 1
       const uint32_t hstep = __ldg(&g_cls[sid].hash_step);
       pos = next_probe(first, 0, ncib, nchunks, mn, hstep, mod_magic(mm.z, mm.w));
@@ -809,14 +1020,19 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
   if (reserved) {
     bool crossed;
     if (commit(rmask, sb, ncib, cid, __ldg(&g_cls[sid].busy), pos, block, crossed)) {
+      HA_STAMP(kStMallocCount, crossed);
       p = publish(sb, pos, enc, ncib);
       flags = crossed ? kNeedHead : 0;
     } else {
       flags = kWant | kNeedHead;
     }
   }
-  if (__any_sync(warp, flags != 0))
-    p = malloc_slow(warp, hbase, nbytes, ticket, sb, pos, round, flags, p);
+  if (__any_sync(warp, flags != 0)) {
+    HA_STAMP(kStSlowIn, flags);
+    p = malloc_slow(warp, hs, nbytes, ticket, sb, pos, round, flags, p);
+    HA_STAMP(kStSlowOut, (uint32_t)(uintptr_t)p);
+  }
+  HA_STAMP(kStMallocOut, (uint32_t)(uintptr_t)p);
   return p;
 }
 
@@ -827,26 +1043,30 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
 __device__ __forceinline__ void free_small(uint64_t off) {
   const uint32_t sb = (uint32_t)(off >> c_cfg.sb_sh);
   const uint32_t in = (uint32_t)off & ((1u << c_cfg.sb_sh) - 1u);
+  HA_STAMP(kStFreeIn, in);
   // independent loads: the block's nibble (taken and cleared) and the
   // slab's chunk size
   uint32_t *nw = &nibs_of(sb)[in >> 7];
   const uint32_t sh = (in >> 2) & 28;
   const uint32_t enc = ld_relaxed(&g_st.desc[sb].chunk_enc);
-  const uint32_t old = atom_and(nw, ~(15u << sh));
+  const uint32_t old = atom_and_meta(nw, ~(15u << sh));
   const uint32_t n = (old >> sh) & 15u;
+  HA_STAMP(kStFreeNibble, old ^ enc);
   const bool valid = n != 0 && enc != 0;
   if (!valid) raise_status(HA_ST_BAD_FREE);
   const uint32_t ichunk = valid ? chunk_div(in, enc) : 0;
-  if (valid) red_and(&bits_of(sb)[ichunk >> 5], ~(((1u << n) - 1u) << (ichunk & 31)));
+  if (valid) red_and_meta(&bits_of(sb)[ichunk >> 5], ~(((1u << n) - 1u) << (ichunk & 31)));
   const uint32_t vmask = __ballot_sync(__activemask(), valid);
   if (valid) {
     const uint32_t grp = __match_any_sync(vmask, sb);
     const uint32_t total = __reduce_add_sync(grp, n);
     if (lane_id() == (uint32_t)(__ffs(grp) - 1)) {
-      const uint32_t before = atom_add(ctr_of(sb), 0u - (total << kCntShift));
+      const uint32_t before = atom_add_meta(ctr_of(sb), 0u - (total << kCntShift));
+      HA_STAMP(kStFreeCount, before);
       if (!(before & kHeadFlag)) file_after_free(sb, before, total);
     }
   }
+  HA_STAMP(kStFreeOut, vmask);
 }
 
 }  // namespace ha

@@ -15,6 +15,7 @@
 
 #include "halloc.h"
 #include "halloc_c.h"
+#include "ha_stamp.cuh"  // HA_STAMP (a no-op unless built with -DHA_STAMPS)
 #include "ha_hist.cuh"
 
 namespace {
@@ -131,6 +132,7 @@ __device__ __forceinline__ void throughput_thread(uint32_t i, uint32_t sz, uint3
       void *p = ps[a];
       if (!p) continue;
       const uint4 v = load16(p);
+      HA_STAMP(ha::kStUser, v.x);
       sum += (unsigned long long)v.x + v.y + v.z + v.w;
       if (kCudaHeap)
         free(p);
@@ -148,6 +150,20 @@ __global__ void ha_throughput_k(const uint32_t *sizes, uint32_t nbytes, uint32_t
   unsigned long long sum = 0, nfail = 0;
   if (i < n) throughput_thread<kCudaHeap>(i, sizes ? sizes[i] : nbytes, nallocs, niters, sum, nfail);
   block_add2(sum, nfail, out, out + 1);
+}
+
+// The private-throughput loop run by one warp with the latency stamps of an
+// HA_STAMPS build switched on (kStampBytes of dynamic shared memory); the
+// stamps are copied to out (kStampBytes / 4 words) at the end.
+__global__ void ha_stamps_k(uint32_t nbytes, uint32_t niters, uint32_t *out) {
+#ifdef HA_STAMPS
+  ha::ha_stamp_smem[threadIdx.x] = 0;
+  __syncwarp();
+  unsigned long long sum = 0, nfail = 0;
+  throughput_thread<false>(threadIdx.x, nbytes, 1, niters, sum, nfail);
+  __syncwarp();
+  for (uint32_t i = threadIdx.x; i < ha::kStampBytes / 4; i += 32) out[i] = ha::ha_stamp_smem[i];
+#endif
 }
 
 // Totals of the mapped-transfer loop while its blocks run; the last block
@@ -1341,6 +1357,18 @@ extern "C" int ha_batched_run_noalloc_c(const ha_batch_plan_t *plan, uint32_t bl
       reinterpret_cast<unsigned long long *>(plan->req_ptr), plan->free_ids,
       reinterpret_cast<unsigned int *>(scratch + kNaCtlOff), acc);
   return launch_status();
+}
+
+extern "C" int ha_stamps_run_c(uint32_t nbytes, uint32_t niters, uint32_t *d_out,
+                               void *stream) {
+#ifdef HA_STAMPS
+  if (!d_out || niters == 0 || nbytes == 0 || nbytes > 3072) return HA_EINVAL;
+  ha_stamps_k<<<1, 32, ha::kStampBytes, as_stream(stream)>>>(nbytes, niters, d_out);
+  return launch_status();
+#else
+  (void)nbytes, (void)niters, (void)d_out, (void)stream;
+  return HA_ESTATE;  // a normal build records no stamps
+#endif
 }
 
 extern "C" int ha_trace_c(const int64_t *ops, int64_t n, int64_t *out, void *stream) {

@@ -123,6 +123,28 @@ uint32_t heads_for_init() {
 }
 // bytes backed at the next init, 0 = the whole pool (no growth)
 uint64_t g_growth_initial = 0;
+// surge head sets for the next init: -1 = from HALLOC_SURGE (default on)
+int g_surge = -1;
+
+// Whether an init with `nheads` head slabs per size opens surge head sets
+// under contention: only with the single head of the reference policy.  A
+// program written against halloc.h alone turns them off with HALLOC_SURGE=0
+// in its environment; an ha_set_surge_c call wins.
+uint32_t surge_for_init(uint32_t nheads) {
+  if (nheads != 1) return 0;
+  if (g_surge >= 0) return (uint32_t)g_surge;
+  const char *e = getenv("HALLOC_SURGE");
+  if (!e || !*e) return 1;
+  if (!strcmp(e, "0")) return 0;
+  if (!strcmp(e, "1")) return 1;
+  fprintf(stderr, "halloc-b200: HALLOC_SURGE=%s ignored (0 or 1)\n", e);
+  return 1;
+}
+
+uint32_t decode_head(uint32_t w) {
+  const uint32_t sb = w & ha::kSlabField;
+  return sb == ha::kSlabField ? ha::kNone : sb;
+}
 
 #define HA_CK(call)                                   \
   do {                                                \
@@ -434,7 +456,7 @@ int init_impl(const ha_opts_c &o) {
     memset(st, 0, sizeof(*st));
     for (uint32_t s = 0; s < ha::kMaxHeads * ha::kNSizes; s++) {
       st->ticket[s * ha::kTicketStride] = ha::kFirstTicket;
-      st->head[s] = ha::kNone;
+      st->head[s] = ha::kSlabField;  // no head, surge level 0
       st->cached[s] = ha::kNone;
     }
     st->wait_limit_us = ha::kDefaultWaitUs;
@@ -460,6 +482,7 @@ int init_impl(const ha_opts_c &o) {
     cfg.set_words = (uint32_t)((nsbs + 31) / 32);
     cfg.sum_words = (cfg.set_words + 31) / 32;
     cfg.nheads = heads_for_init();
+    cfg.surge = surge_for_init(cfg.nheads);
     cfg.growth = grow.growth ? 1 : 0;
     if (cudaMemset(meta, 0, meta_bytes) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_cls, cls, sizeof(cls)) != cudaSuccess ||
@@ -699,7 +722,7 @@ extern "C" int ha_stats_c(ha_stats_t *out) {
   ha::StatsOut s;
   int rc = run_stats(0, &s);
   if (rc) return rc;
-  uint32_t head[ha::kNSizes], cached[ha::kNSizes], misc[5];
+  uint32_t head[ha::kNSizes], cached[ha::kNSizes], misc[6];
   HA_CK(cudaMemcpyFromSymbol(head, ha::g_st, sizeof(head), offsetof(ha::State, head)));
   HA_CK(cudaMemcpyFromSymbol(cached, ha::g_st, sizeof(cached), offsetof(ha::State, cached)));
   HA_CK(cudaMemcpyFromSymbol(misc, ha::g_st, sizeof(misc), offsetof(ha::State, status)));
@@ -717,8 +740,12 @@ extern "C" int ha_stats_c(ha_stats_t *out) {
   out->n_head_changes = misc[2];
   out->n_null = misc[3];
   out->heap_limit_ok = h->heap_ok ? 1 : 0;
-  memcpy(out->head, head, sizeof(head));
+  for (uint32_t k = 0; k < ha::kNSizes; k++) {
+    out->head[k] = decode_head(head[k]);
+    out->surge_level[k] = head[k] >> ha::kLevelShift;
+  }
   memcpy(out->cached, cached, sizeof(cached));
+  out->n_surge_changes = misc[5];
   out->growth = h->growth ? 1 : 0;
   out->committed_slabs = misc[4];
   out->unit_bytes = h->unit_bytes;
@@ -866,7 +893,7 @@ extern "C" int ha_dump_state_c(const ha_state_dump_t *d) {
   const uint32_t n = h->nsbs, nw = (n + 31) / 32;
   for (uint32_t s = 0; s < ha::kNSizes; s++) {
     if (d->tickets) d->tickets[s] = st->ticket[s * ha::kTicketStride];
-    if (d->heads) d->heads[s] = st->head[s];
+    if (d->heads) d->heads[s] = decode_head(st->head[s]);
     if (d->cached) d->cached[s] = st->cached[s];
   }
   for (uint32_t sb = 0; sb < n; sb++) {
@@ -893,6 +920,12 @@ extern "C" int ha_set_heads_c(uint32_t nheads) {
   if (nheads == 0 || nheads > ha::kMaxHeads || (nheads & (nheads - 1))) return HA_EINVAL;
   g_nheads = nheads;
   g_nheads_set = true;
+  return HA_OK;
+}
+
+extern "C" int ha_set_surge_c(int on) {
+  if (on < -1 || on > 1) return HA_EINVAL;
+  g_surge = on;
   return HA_OK;
 }
 

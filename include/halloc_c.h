@@ -83,6 +83,9 @@ typedef struct ha_stats_t {
   uint32_t growth;          /* 1 when the pool grows on demand (ha_set_growth_c) */
   uint32_t committed_slabs; /* slabs backed by device memory (nsbs without growth) */
   uint64_t unit_bytes;      /* growth / release unit, a multiple of the slab size */
+  uint32_t surge_level[16]; /* per size class: 2^level head sets open (0 = one) */
+  uint32_t n_surge_changes; /* surge level changes since init */
+  uint32_t reserved;
 } ha_stats_t;
 
 /* Fills *out (synchronises the device).  No counterpart in the reference,
@@ -157,6 +160,23 @@ int ha_set_hash_scale_c(uint32_t percent);
    with HALLOC_HEADS=<n> in its environment, read at init; a call here wins
    over the environment. */
 int ha_set_heads_c(uint32_t nheads);
+
+/* Surge head sets (on by default with one head per size; applied by the
+   next init on this process).  When thousands of warps queue for one size's
+   head replacement during one head's life (kSurgeUp = 2,048 queued warps: a
+   grid of 1,024 warps can never get there), the size gets 2, then 4, then
+   8 head slabs, each serving the SMs whose id modulo the set count names
+   it; the sets close again one level per head change that saw fewer than
+   256 queued warps, and all of them at once when the size runs short of
+   slabs, so a NULL still means that no slab is left for the size.  A thread
+   alone, or any grid that never queues that many warps, keeps the
+   reference policy's single head and addresses.  0 turns them off (the
+   reference policy under every load), 1 on, -1 back to the environment's
+   choice; HALLOC_SURGE=0|1 in the environment does the same for programs
+   that only use halloc.h.  Ignored
+   when ha_set_heads_c chose more than one head.  No counterpart in the
+   reference (halloc src/slab.cuh:378-445 has one head per size). */
+int ha_set_surge_c(int on);
 
 /* Test hook for failure detection: sets the head-replacement lock of size
    class `size_id` to `held` (1 = held by a holder that never releases it,
@@ -498,6 +518,20 @@ typedef struct ha_serve_result_t {
 
 int ha_serve_run_c(const ha_serve_cfg_t *cfg, ha_serve_result_t *out,
                    void *stream);
+
+/* Latency breakdown of one warp (instrumented builds only): runs the
+   private-throughput loop (hamalloc(nbytes), 16-byte write and read-back,
+   hafree; niters iterations) with 32 threads, and copies to d_out (device,
+   10,272 words) the SM clock each lane read after every dependent round
+   trip of hamalloc / hafree: word l = lane l's stamp count, then 2 words
+   per stamp (point id, clock low word) at 32 + 2 * (l * 160 + i).  Point
+   ids: 1 hamalloc entered, 2 ticket and head back, 3 bit reservation back,
+   4 slab count back, 5 hamalloc returns, 6/7 slow path in/out, 8 hafree
+   entered, 9 size nibble and descriptor back, 10 count-down back, 11 hafree
+   returns, 12 payload read back.  HA_ESTATE in a normal build: only the
+   library built with -DHA_STAMPS (halloc_b200/build.py, stamps=True)
+   records them.  No counterpart in the reference. */
+int ha_stamps_run_c(uint32_t nbytes, uint32_t niters, uint32_t *d_out, void *stream);
 
 /* Replays a trace on ONE device thread: op >= 0 is hamalloc(op);
    op < 0 is hafree of the block returned by op index -(op + 1).

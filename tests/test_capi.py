@@ -51,7 +51,7 @@ def test_options_layout_matches_halloc_opts_t():
 
 
 def test_stats_layout():
-    assert ctypes.sizeof(H._CStats) == 5 * 8 + 8 * 4 + 32 * 4 + 2 * 4 + 8
+    assert ctypes.sizeof(H._CStats) == 5 * 8 + 8 * 4 + 32 * 4 + 2 * 4 + 8 + 16 * 4 + 2 * 4
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):

@@ -371,6 +371,7 @@ def test_heads_from_environment(torch_cuda, env, many):
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     e = dict(os.environ)
     e.pop("HALLOC_HEADS", None)
+    e["HALLOC_SURGE"] = "0"  # fixed heads only: no surge sets under this storm
     if env is not None:
         e["HALLOC_HEADS"] = env
     r = subprocess.run([sys.executable, "-c", _HEADS_PROBE.format(root=root)], env=e,

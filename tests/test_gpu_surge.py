@@ -1,0 +1,123 @@
+"""Surge head sets (ha_set_surge_c): under a storm -- thousands of warps
+queueing for one size's head replacement -- a size gets 2, 4 or 8 head
+slabs, and gives them back as the queue shrinks or slabs run short.
+
+Checked here: a storm opens sets and every result stays exact (payload
+checksums, no overlap, quiescent per-slab state equal to what the live
+blocks imply, every slab back in the free set or a head after the last
+free); the plain 32,768-thread workload never opens one; with surge sets off
+a storm keeps the single head; and a storm that exhausts the pool gets as
+many blocks as the single-head policy does (NULL still means no slab is
+left).  The serial-trace parity tests run with surge sets on (the default)
+and show that a lone thread never opens one.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import allocator, check_blocks, plain_checksum
+from tests.test_gpu_concurrent import assert_empty, assert_state_matches_live, malloc_batch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def surge_default():
+    """Leaves the surge knob at the environment's choice afterwards."""
+    import halloc_b200 as H
+    yield H
+    H.set_surge(None)
+
+
+def run_loop(torch, H, n, nbytes, nallocs=1, niters=2, block=256):
+    out = torch.zeros(2, dtype=torch.int64, device="cuda")
+    H.throughput(out, n, nbytes=nbytes, block=block, nallocs=nallocs, niters=niters)
+    torch.cuda.synchronize()
+    return out.cpu().tolist()
+
+
+def test_storm_opens_surge_sets_and_stays_exact(torch_cuda, surge_default):
+    torch = torch_cuda
+    n = 1 << 20
+    with allocator(memory=1 << 30) as H:
+        assert run_loop(torch, H, n, 256) == [plain_checksum(n, 2), 0]
+        st = H.stats()
+        assert st["n_surge_changes"] > 0
+        assert st["used_chunks"] == 0 and H.status() == 0
+
+
+def test_blocks_held_under_a_storm(torch_cuda, surge_default):
+    """1 M threads each hold one 256-B block: invariants and the per-slab
+    state hold with surge sets open, and after the last free every slab is
+    in the free set or is a head or prefetched slab."""
+    torch = torch_cuda
+    n = 1 << 20
+    sizes = np.full(n, 256, np.int64)
+    with allocator(memory=1 << 30) as H:
+        st = H.stats()
+        ptrs = malloc_batch(torch, H, sizes, n, 1)
+        p = ptrs.cpu().numpy()
+        check_blocks(p, sizes, st["pool_base"], st["pool_bytes"])
+        assert H.stats()["n_surge_changes"] > 0
+        assert_state_matches_live(H, p, sizes)
+        H.free_batch(ptrs, n, 1)
+        torch.cuda.synchronize()
+        assert_empty(H)
+        st = H.stats()
+        assert st["free_slabs"] + st["head_slabs"] == st["nsbs"]
+        assert H.status() == 0
+
+
+def test_plain_workload_keeps_one_head(torch_cuda, surge_default):
+    """The 32,768-thread plain workload (1,024 warps) never queues enough
+    warps for a head to open a surge set."""
+    torch = torch_cuda
+    n = 32768
+    with allocator(memory=512 << 20) as H:
+        for _ in range(30):
+            assert run_loop(torch, H, n, 16, niters=10, block=128) == [plain_checksum(n, 10), 0]
+        st = H.stats()
+        assert st["n_surge_changes"] == 0 and st["surge_level"] == [0] * 16
+        assert st["n_head_changes"] > 0
+
+
+def test_surge_off_keeps_one_head_under_a_storm(torch_cuda, surge_default):
+    torch = torch_cuda
+    n = 1 << 20
+    H = surge_default
+    H.set_surge(False)
+    with allocator(memory=1 << 30) as H:
+        assert run_loop(torch, H, n, 256) == [plain_checksum(n, 2), 0]
+        st = H.stats()
+        assert st["n_surge_changes"] == 0 and st["surge_level"] == [0] * 16
+        assert st["head_slabs"] <= 2
+
+
+def _exhaust(torch, H, surge: bool):
+    """1 M requests of 256 B (256 MiB) against a 96-MiB slab pool of 2-MiB
+    slabs: returns (blocks handed out, surge level changes)."""
+    n = 1 << 20
+    sizes = np.full(n, 256, np.int64)
+    H.set_surge(surge)
+    with allocator(memory=128 << 20, sb_sz_sh=21) as H:
+        st = H.stats()
+        ptrs = malloc_batch(torch, H, sizes, n, 1)
+        p = ptrs.cpu().numpy()
+        r = check_blocks(p, sizes, st["pool_base"], st["pool_bytes"], allow_null=True)
+        assert_state_matches_live(H, p, sizes)
+        changes = H.stats()["n_surge_changes"]
+        H.free_batch(ptrs, n, 1)
+        torch.cuda.synchronize()
+        assert_empty(H)
+        assert H.status() == 0
+        return r["n"], changes
+
+
+def test_exhaustion_under_a_storm_gets_what_one_head_gets(torch_cuda, surge_default):
+    torch = torch_cuda
+    one, changes_one = _exhaust(torch, surge_default, False)
+    many, changes = _exhaust(torch, surge_default, True)
+    assert changes_one == 0 and changes > 0
+    # one head fills every slab to its busy threshold (83.5 %), then takes
+    # busy slabs up to half way to full; surge heads are filed by occupancy
+    # when their sets close, so the pool ends about as full
+    assert many >= 0.97 * one, (many, one)
