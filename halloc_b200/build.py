@@ -92,23 +92,26 @@ def build_stamps(verbose: bool = False) -> str:
     return STAMPS_SO
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> str:
-    """Compiles what is out of date; returns the path of the shared library."""
+def build(verbose: bool = False, ptxas_info: bool = False, defines=()) -> str:
+    """Compiles what is out of date; returns the path of the shared library.
+    `defines` (e.g. ["HA_L2_HINTS=0"]) rebuilds everything with those macros:
+    a variant build for a measurement, replacing the default one in place."""
     os.makedirs(BUILD, exist_ok=True)
     cc = nvcc()
     objs = []
+    dflags = ["-D" + d for d in defines]
     for src, flags in SOURCES.items():
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
-        if _stale(o, [s, __file__] + HEADERS) or ptxas_info:
+        if _stale(o, [s, __file__] + HEADERS) or ptxas_info or dflags:
             extra = ["-Xptxas", "-v"] if ptxas_info else []
-            _run([cc] + CUFLAGS + flags + extra + ["-c", s, "-o", o], verbose)
+            _run([cc] + CUFLAGS + flags + dflags + extra + ["-c", s, "-o", o], verbose)
         objs.append(o)
     halloc_o = objs[0]
-    if _stale(LIB_A, [halloc_o]):
+    if _stale(LIB_A, [halloc_o]) or dflags:
         _run([cc] + ARCH + ["-lib", halloc_o, "-o", LIB_A], verbose)
     dlink = os.path.join(BUILD, "dlink.o")
-    if _stale(SO, objs):
+    if _stale(SO, objs) or dflags:
         _run([cc] + ARCH + ["-Xcompiler", "-fPIC", "-dlink"] + objs + ["-o", dlink], verbose)
         _run([cc] + ARCH + ["-shared", "-Xcompiler", "-fPIC"] + objs + [dlink, "-o", SO,
                                                                          "-lcudadevrt"],
@@ -132,5 +135,6 @@ def _build_pyfast(verbose: bool) -> None:
 
 
 if __name__ == "__main__":
-    build(verbose=True, ptxas_info="--ptxas" in sys.argv)
+    build(verbose=True, ptxas_info="--ptxas" in sys.argv,
+          defines=[a[2:] for a in sys.argv[1:] if a.startswith("-D")])
     print(SO)

@@ -1363,8 +1363,31 @@ extern "C" int ha_stamps_run_c(uint32_t nbytes, uint32_t niters, uint32_t *d_out
                                void *stream) {
 #ifdef HA_STAMPS
   if (!d_out || niters == 0 || nbytes == 0 || nbytes > 3072) return HA_EINVAL;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    fprintf(stderr, "halloc-b200: error pending before the stamps launch: %s\n",
+            cudaGetErrorString(e));
+  e = cudaFuncSetAttribute(ha_stamps_k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)ha::kStampBytes);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "halloc-b200: stamps kernel attribute: %s\n", cudaGetErrorString(e));
+    return HA_ECUDA;
+  }
   ha_stamps_k<<<1, 32, ha::kStampBytes, as_stream(stream)>>>(nbytes, niters, d_out);
-  return launch_status();
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    cudaFuncAttributes fa;
+    memset(&fa, 0, sizeof(fa));
+    cudaFuncGetAttributes(&fa, ha_stamps_k);
+    cudaGetLastError();
+    fprintf(stderr,
+            "halloc-b200: stamps launch failed: %s (static smem %zu, max dynamic smem %d, "
+            "local %zu, regs %d, max threads %d)\n",
+            cudaGetErrorString(e), fa.sharedSizeBytes, fa.maxDynamicSharedSizeBytes,
+            fa.localSizeBytes, fa.numRegs, fa.maxThreadsPerBlock);
+    return HA_ECUDA;
+  }
+  return HA_OK;
 #else
   (void)nbytes, (void)niters, (void)d_out, (void)stream;
   return HA_ESTATE;  // a normal build records no stamps

@@ -69,7 +69,8 @@ def test_reduced_sweep_on_a_small_plan(torch_cuda):
         return verified[-1]
 
     runner.verify = counting_verify
-    out = A.autotune(torch, runner, memory=256 << 20, halloc_fraction=0.5, reps=1,
+    # 512 MiB of 2-MiB slabs: room for two head sets per size (4 slabs each)
+    out = A.autotune(torch, runner, memory=1 << 30, halloc_fraction=0.5, reps=1,
                      slab_shifts=(21, 22), busy_fractions=(0.835,), blocks=(128, 256),
                      hash_pcts=(100,), heads=(2,))
     # 2 + 1 + 1 points, each verified after its warm-up launch and its replay

@@ -114,3 +114,25 @@ def test_closed_batch_gives_the_streamed_results(torch_cuda):
         assert rb["alloc_failures"] == 0 and rb["timeouts"] == 0
         assert torch.equal(a, b)
         assert H.stats()["used_chunks"] == 0 and H.status() == 0
+
+
+def test_serving_at_the_benchmark_rate(torch_cuda):
+    """One point of the benchmark's sweep: 1 M jobs at lambda = 1e8 jobs/s,
+    256-B blocks, job lengths log-uniform 64 B..2 MiB, 16 GiB pool.  Every
+    job completes with no failure or timeout, the latency histogram holds
+    every allocation, a sample of jobs' value sums equals the host
+    recomputation, and the pool is empty at the end."""
+    import halloc_b200 as H
+    torch = torch_cuda
+    n = 1_000_000
+    with allocator(memory=16 << 30):
+        res = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+        r = H.serve_run(res, n, 1e8, seed=7)
+        assert r["jobs_done"] == n and r["alloc_failures"] == 0 and r["timeouts"] == 0
+        assert int(r["hist"].sum()) == r["allocs"] and r["allocs"] > 100 * n
+        assert r["p99_cycles"] >= r["p50_cycles"] > 0
+        got = res.view(-1, 2).cpu().numpy().astype(np.uint64)
+        ids = np.random.default_rng(3).choice(n, 300, replace=False)
+        assert np.array_equal(got[ids, 1], value_sums(ids, got[ids, 0]))
+        st = H.stats()
+        assert st["used_chunks"] == 0 and st["status"] == 0
