@@ -69,7 +69,7 @@ STAMPS_SO = os.path.join(PKG, "libhalloc_b200_stamps.so")
 STAMPS_BUILD = os.path.join(PKG, "_build_stamps")
 
 
-def build_stamps(verbose: bool = False) -> str:
+def build_stamps(verbose: bool = False, defines=()) -> str:
     """The instrumented library (-DHA_STAMPS): the allocator and the batch
     kernels with latency stamps after every dependent round trip of
     hamalloc / hafree (see csrc/ha_stamp.cuh).  Used only by
@@ -77,14 +77,16 @@ def build_stamps(verbose: bool = False) -> str:
     os.makedirs(STAMPS_BUILD, exist_ok=True)
     cc = nvcc()
     objs = []
+    dflags = ["-D" + d for d in defines]
     for src in ("halloc.cu", "ha_kernels.cu"):
         s = os.path.join(CSRC, src)
         o = os.path.join(STAMPS_BUILD, src.replace(".cu", ".o"))
-        if _stale(o, [s, __file__] + HEADERS):
-            _run([cc] + CUFLAGS + SOURCES[src] + ["-DHA_STAMPS", "-c", s, "-o", o], verbose)
+        if _stale(o, [s, __file__] + HEADERS) or dflags:
+            _run([cc] + CUFLAGS + SOURCES[src] + dflags + ["-DHA_STAMPS", "-c", s, "-o", o],
+                 verbose)
         objs.append(o)
     dlink = os.path.join(STAMPS_BUILD, "dlink.o")
-    if _stale(STAMPS_SO, objs):
+    if _stale(STAMPS_SO, objs) or dflags:
         _run([cc] + ARCH + ["-Xcompiler", "-fPIC", "-dlink"] + objs + ["-o", dlink], verbose)
         _run([cc] + ARCH + ["-shared", "-Xcompiler", "-fPIC"] + objs + [dlink, "-o", STAMPS_SO,
                                                                          "-lcudadevrt"],
@@ -117,7 +119,7 @@ def build(verbose: bool = False, ptxas_info: bool = False, defines=()) -> str:
                                                                          "-lcudadevrt"],
              verbose)
     _build_pyfast(verbose)
-    build_stamps(verbose)
+    build_stamps(verbose, defines)
     return SO
 
 
