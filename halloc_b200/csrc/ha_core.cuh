@@ -692,12 +692,23 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
       return none;
     }
     if (set == 0 && c_cfg.surge && nlevel == level) {
-      // how many warps queued for this size's heads during the old head's
-      // life: open a level above kSurgeUp, close one below kSurgeDown
-      const uint32_t storm = atomicExch(&g_st.storm[sid * kTicketStride], 0u);
-      if (storm >= kSurgeUp && level < kMaxLevel)
+      // How many warps queued for this size's heads during the old head's
+      // life, and how many tickets set 0 gave out meanwhile (about the
+      // allocations its head served).  Open a level when the queue is a
+      // storm (kSurgeUp), or when it is long and the head served only a few
+      // allocations per queued warp of its set (a head too small for the
+      // grid: kSurgeTicketsUp each); close one when neither comes near.
+      uint32_t *line = &g_st.storm[sid * kTicketStride];
+      const uint32_t storm = atomicExch(line, 0u);
+      const uint32_t tnow = ld_relaxed(&g_st.ticket[sid * kTicketStride]);
+      const uint32_t tickets = tnow - ld_relaxed(line + 1);
+      st_relaxed(line + 1, tnow);
+      const uint32_t per_set = storm >> level;
+      const bool crowded = per_set >= kSurgeQueueMin && tickets < kSurgeTicketsUp * per_set;
+      const bool calm = per_set < kSurgeQueueMin / 4 || tickets >= kSurgeTicketsDown * per_set;
+      if ((storm >= kSurgeUp || crowded) && level < kMaxLevel)
         nlevel = level + 1;
-      else if (storm < kSurgeDown && level > 0)
+      else if (storm < kSurgeDown && calm && level > 0)
         nlevel = level - 1;
     }
     st_release(head, head_word(next, nlevel));
@@ -1040,94 +1051,33 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
 // block's offset from the start of the pool.  (halloc src/halloc.cu:211-230)
 // Block starts are at least 16 B apart (24-B chunks start on 8-B
 // boundaries), so in-slab offset / 16 names a block start uniquely.
-//
-// The count-down is speculative where the slab serves a size of one chunk
-// per block (16, 24, 256 or 384 B, read from an L1-cached copy of the slab's
-// descriptor, a hint only): one chunk per lane leaves in the same round trip
-// as the nibble take, so such a free is one dependent round trip instead of
-// two.  Every block holds at least one chunk, so a valid free never takes
-// the count below its true value.  Once the nibble is back, the group's
-// leader settles the difference (more chunks, or a free that was not a live
-// block) with a second atomic and files the slab from the count before the
-// first as if the whole change were one atomic: a lone thread makes the
-// reference's decisions exactly.  An invalid free (a double free) takes the
-// count one chunk too low until it is settled; a valid free of the same slab
-// that runs in that window and sees the count reach zero releases the slab
-// with one block still live.  Programs that never free a block twice, or
-// that free twice from one thread at a time, cannot meet that window.
-// Build with -DHA_SPEC_FREE=0 for the two-round-trip free everywhere.
-#ifndef HA_SPEC_FREE
-#define HA_SPEC_FREE 1
-#endif
-__device__ __forceinline__ uint32_t single_chunk_hint(uint32_t sb) {
-#if HA_SPEC_FREE
-  // sizes whose blocks are one chunk: 16, 24, 256, 384 B (classes 0, 1, 8, 9)
-  const uint32_t sid = __ldca(&g_st.desc[sb].size_id);
-  return sid < kNSizes && (sid & 6u) == 0u;
-#else
-  return 0u;
-#endif
-}
 __device__ __forceinline__ void free_small(uint64_t off) {
   const uint32_t sb = (uint32_t)(off >> c_cfg.sb_sh);
   const uint32_t in = (uint32_t)off & ((1u << c_cfg.sb_sh) - 1u);
   HA_STAMP(kStFreeIn, in);
-  const uint32_t active = __activemask();
+  // independent loads: the block's nibble (taken and cleared) and the
+  // slab's chunk size
   uint32_t *nw = &nibs_of(sb)[in >> 7];
   const uint32_t sh = (in >> 2) & 28;
-  // in flight first: the block's nibble (taken and cleared) and the slab's
-  // chunk size
   const uint32_t enc = ld_relaxed(&g_st.desc[sb].chunk_enc);
   const uint32_t old = atom_and_meta(nw, ~(15u << sh));
-  // speculative group: lanes whose slab's hint says one chunk per block
-  const bool spec = single_chunk_hint(sb);
-  const uint32_t smask = __ballot_sync(active, spec);
-  uint32_t sgrp = 0, spec_before = 0;
-  if (spec) {
-    sgrp = __match_any_sync(smask, sb);
-    if (lane_id() == (uint32_t)(__ffs(sgrp) - 1))
-      spec_before = atom_add_meta(ctr_of(sb), 0u - ((uint32_t)__popc(sgrp) << kCntShift));
-  }
   const uint32_t n = (old >> sh) & 15u;
   HA_STAMP(kStFreeNibble, old ^ enc);
   const bool valid = n != 0 && enc != 0;
   if (!valid) raise_status(HA_ST_BAD_FREE);
   const uint32_t ichunk = valid ? chunk_div(in, enc) : 0;
   if (valid) red_and_meta(&bits_of(sb)[ichunk >> 5], ~(((1u << n) - 1u) << (ichunk & 31)));
-  const uint32_t nv = valid ? n : 0u;
-  // a group leader's filing, done by one call at the end (a lane leads at
-  // most one group): nothing is live across it
-  uint32_t fbefore = 0, ftotal = 0;
-  if (spec) {
-    // settle the speculative group: its chunks (valid lanes) against its
-    // lanes (one chunk each, already taken off)
-    const uint32_t total = __reduce_add_sync(sgrp, nv);
-    const uint32_t lanes = __popc(sgrp);
-    if (lane_id() == (uint32_t)(__ffs(sgrp) - 1)) {
-      HA_STAMP(kStFreeCount, spec_before);
-      uint32_t before = spec_before;
-      if (total != lanes) {
-        // the rest (or the give-back) as a second atomic; the count the
-        // group saw is the one before it, plus what the first took off
-        before = atom_add_meta(ctr_of(sb), (lanes - total) << kCntShift) +
-                 (lanes << kCntShift);
-      }
-      fbefore = before;
-      ftotal = total;
-    }
-  }
-  const uint32_t vmask = __ballot_sync(active, valid && !spec);
-  if (valid && !spec) {
+  const uint32_t vmask = __ballot_sync(__activemask(), valid);
+  if (valid) {
     const uint32_t grp = __match_any_sync(vmask, sb);
     const uint32_t total = __reduce_add_sync(grp, n);
     if (lane_id() == (uint32_t)(__ffs(grp) - 1)) {
-      fbefore = atom_add_meta(ctr_of(sb), 0u - (total << kCntShift));
-      HA_STAMP(kStFreeCount, fbefore);
-      ftotal = total;
+      const uint32_t before = atom_add_meta(ctr_of(sb), 0u - (total << kCntShift));
+      HA_STAMP(kStFreeCount, before);
+      if (!(before & kHeadFlag)) file_after_free(sb, before, total);
     }
   }
-  HA_STAMP(kStFreeOut, vmask | smask);
-  if (ftotal && !(fbefore & kHeadFlag)) file_after_free(sb, fbefore, ftotal);
+  HA_STAMP(kStFreeOut, vmask);
 }
 
 }  // namespace ha

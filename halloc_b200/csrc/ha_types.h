@@ -58,6 +58,17 @@ constexpr uint32_t kRedirect = 0xfffffffeu;  // replace_head: use head set 0
 // of one head of set 0 (a grid of 1,024 warps can never reach it)
 constexpr uint32_t kSurgeUp = 2048;
 constexpr uint32_t kSurgeDown = 256;
+// second trigger (off unless built with HA_SURGE_TICKETS_UP > 0): at least
+// kSurgeQueueMin warps queued per open set while the head served fewer than
+// kSurgeTicketsUp allocations per queued warp (P: 1,024 warps at most against
+// a 218,890-block head); closing needs kSurgeTicketsDown per queued warp or a
+// short queue
+#ifndef HA_SURGE_TICKETS_UP
+#define HA_SURGE_TICKETS_UP 0  // 0: the second trigger is off
+#endif
+constexpr uint32_t kSurgeQueueMin = 128;
+constexpr uint32_t kSurgeTicketsUp = HA_SURGE_TICKETS_UP;
+constexpr uint32_t kSurgeTicketsDown = 4 * HA_SURGE_TICKETS_UP;
 
 // size class, 32 bytes, the field order of halloc src/size-info.h:8-26
 struct alignas(32) Class {
