@@ -591,6 +591,35 @@ __device__ __noinline__ bool surge_slabs_held(uint32_t sid) {
   return any;
 }
 
+// Closes the surge sets of every size but `own` that holds slabs in them, so
+// that a search that found nothing can look again: a size that went quiet
+// keeps its level until its own next head change, and its surge heads would
+// otherwise hold slabs other sizes need.  A size whose set-0 lock is free
+// gets level 0 written into its head word first (no warp opens its sets
+// again); one whose lock is busy has its sets emptied all the same.  The
+// set-0 lock of another size is only tried, never waited for.  Returns
+// whether any slab was filed.
+__device__ __noinline__ bool close_other_surges(uint32_t own) {
+  bool any = false;
+  for (uint32_t sid = 0; sid < kNSizes; sid++) {
+    if (sid == own || !surge_slabs_held(sid)) continue;
+    uint32_t *hlock0 = &g_st.head_lock[sid * kTicketStride];
+    bool closed = false;
+    if (ld_relaxed(hlock0) == 0 && try_lock(hlock0)) {
+      const uint32_t w = ld_relaxed(&g_st.head[sid]);
+      if (head_level(w) != 0) {
+        st_release(&g_st.head[sid], head_word(head_slab(w), 0));
+        red_add(&g_st.n_surge_changes, 1);
+      }
+      unlock(hlock0);
+      closed = true;
+    }
+    for (uint32_t k = 1; k < kMaxHeads; k++) retire_set(k * kNSizes + sid, !closed);
+    any = true;
+  }
+  return any;
+}
+
 // Hands a slab taken for head slot hs back to hs's prefetch slot, or, when
 // another prefetch landed there first, files it again.
 __device__ __noinline__ void hand_back(uint32_t hs, uint32_t sb) {
@@ -685,6 +714,8 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
       nlevel = 0;
       next = find_slab(sid);
     }
+    if (next == kNone && set == 0 && c_cfg.surge && close_other_surges(sid))
+      next = find_slab(sid);
     if (next == kNone) {
       st_relaxed(&g_st.no_slab[hs], epoch + 1u);
       if (nlevel != level) st_release(head, head_word(cur, nlevel));

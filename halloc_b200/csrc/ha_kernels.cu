@@ -220,7 +220,10 @@ __device__ __forceinline__ uint32_t slot_hash(uint32_t seed, uint32_t i, uint32_
 
 // A block's payload: the words base, base+1, ... over its sz bytes (sz a
 // multiple of 8), written with 16-byte stores where the block's address and
-// size allow them (every size but 24 B); returns the sum of the words.
+// size allow them (every size but 24 B); returns the sum of the words.  The
+// stores are streaming (evict-first): a payload is read back only rounds
+// later, and left at normal priority the 1.2 GB of payload sectors an
+// allocation round writes push the allocator's metadata out of L2.
 __device__ __forceinline__ unsigned long long write_pattern(void *p, uint32_t sz,
                                                             uint32_t base) {
   unsigned long long sum = 0;
@@ -229,7 +232,7 @@ __device__ __forceinline__ unsigned long long write_pattern(void *p, uint32_t sz
     for (uint32_t w = 0; w < sz / 16; w++) {
       const uint32_t a = base + 4 * w;
       const uint4 v = make_uint4(a, a + 1, a + 2, a + 3);  // 32-bit words, wrapping
-      q[w] = v;
+      __stcs(q + w, v);
       sum += (unsigned long long)v.x + v.y + v.z + v.w;
     }
   } else {
@@ -237,7 +240,7 @@ __device__ __forceinline__ unsigned long long write_pattern(void *p, uint32_t sz
     for (uint32_t w = 0; w < sz / 8; w++) {
       const uint32_t a = base + 2 * w;
       const uint2 v = make_uint2(a, a + 1);
-      q[w] = v;
+      __stcs(q + w, v);
       sum += (unsigned long long)v.x + v.y;
     }
   }
@@ -246,20 +249,21 @@ __device__ __forceinline__ unsigned long long write_pattern(void *p, uint32_t sz
 
 // The sum of a block's words, read with 16-byte loads where possible and
 // eight loads in flight: the read-back waits on DRAM about once per block.
+// The loads are streaming too: this is the payload's last use.
 __device__ __forceinline__ unsigned long long read_sum(const void *p, uint32_t sz) {
   unsigned long long sum = 0;
   if ((((uintptr_t)p | sz) & 15u) == 0) {
     const uint4 *q = reinterpret_cast<const uint4 *>(p);
 #pragma unroll 8
     for (uint32_t w = 0; w < sz / 16; w++) {
-      const uint4 v = __ldcg(q + w);
+      const uint4 v = __ldcs(q + w);
       sum += (unsigned long long)v.x + v.y + v.z + v.w;
     }
   } else {
     const uint2 *q = reinterpret_cast<const uint2 *>(p);
 #pragma unroll 8
     for (uint32_t w = 0; w < sz / 8; w++) {
-      const uint2 v = __ldcg(q + w);
+      const uint2 v = __ldcs(q + w);
       sum += (unsigned long long)v.x + v.y;
     }
   }

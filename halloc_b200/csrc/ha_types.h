@@ -64,7 +64,7 @@ constexpr uint32_t kSurgeDown = 256;
 // a 218,890-block head); closing needs kSurgeTicketsDown per queued warp or a
 // short queue
 #ifndef HA_SURGE_TICKETS_UP
-#define HA_SURGE_TICKETS_UP 0  // 0: the second trigger is off
+#define HA_SURGE_TICKETS_UP 96  // 0 turns the second trigger off
 #endif
 constexpr uint32_t kSurgeQueueMin = 128;
 constexpr uint32_t kSurgeTicketsUp = HA_SURGE_TICKETS_UP;
