@@ -28,7 +28,7 @@ __all__ = [
     "strings_check", "graph_build", "graph_gather", "serve_run",
     "throughput", "throughput_host", "cuda_throughput", "trace",
     "atomic_peak", "debug_set_head_lock", "set_hash_scale", "set_heads", "set_surge",
-    "set_growth", "grow",
+    "close_surges", "set_growth", "grow",
     "trim", "ST_GROW", "library_path", "load", "ST_TIMEOUT", "ST_BAD_FREE", "ST_LIVELOCK",
 ]
 
@@ -148,6 +148,7 @@ _SIGS = {
     "ha_set_hash_scale_c": (_int, [_u32]),
     "ha_set_heads_c": (_int, [_u32]),
     "ha_set_surge_c": (_int, [ctypes.c_int]),
+    "ha_close_surges_c": (_int, [ctypes.c_void_p]),
     "ha_set_growth_c": (_int, [ctypes.c_uint64]),
     "ha_grow_c": (_int, [ctypes.c_uint64, _vp, ctypes.POINTER(ctypes.c_uint64)]),
     "ha_trim_c": (_int, [ctypes.c_uint64, _vp, ctypes.POINTER(ctypes.c_uint64)]),
@@ -315,6 +316,11 @@ def set_surge(on) -> None:
     """Surge head sets for the next init (see ha_set_surge_c): True, False, or
     None for the environment's choice (HALLOC_SURGE, on by default)."""
     _check(load().ha_set_surge_c(-1 if on is None else (1 if on else 0)), "ha_set_surge_c")
+
+
+def close_surges(stream=None) -> None:
+    """Closes every size's surge head sets (see ha_close_surges_c)."""
+    _check(load().ha_close_surges_c(_stream(stream)), "ha_close_surges_c")
 
 
 def debug_set_head_lock(size_id: int, held: bool) -> None:

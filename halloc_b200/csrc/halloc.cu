@@ -569,6 +569,26 @@ __global__ void ha_adopt_k(uint32_t first, uint32_t count) {
 // when all of them were there and are empty, non-head slabs with no chunk
 // size, and when it fits in max_slabs; otherwise the slabs taken go back.
 // Released chunks are listed in g_trim_out[0 .. g_trim_n).
+// Closes every size's surge head sets (ha_close_surges_c): level 0 in each
+// size's set-0 head word, then the heads and prefetched slabs of sets 1..
+// filed by occupancy.  One thread; every lock wait is bounded.
+__global__ void ha_close_surges_k() {
+  using namespace ha;
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (uint32_t sid = 0; sid < kNSizes; sid++) {
+    uint32_t *hlock0 = &g_st.head_lock[sid * kTicketStride];
+    if (lock(hlock0)) {
+      const uint32_t w = ld_relaxed(&g_st.head[sid]);
+      if (head_level(w) != 0) {
+        st_release(&g_st.head[sid], head_word(head_slab(w), 0));
+        red_add(&g_st.n_surge_changes, 1);
+      }
+      unlock(hlock0);
+    }
+    for (uint32_t k = 1; k < kMaxHeads; k++) retire_set(k * kNSizes + sid, true);
+  }
+}
+
 __global__ void ha_trim_k(uint32_t ncand, uint32_t max_slabs) {
   using namespace ha;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -791,6 +811,15 @@ extern "C" int ha_grow_c(uint64_t bytes, void *stream, uint64_t *added_bytes) {
   return HA_OK;
 }
 
+extern "C" int ha_close_surges_c(void *stream) {
+  HostDev *h = current();
+  if (!h) return HA_ECUDA;
+  if (!h->init) return HA_ESTATE;
+  ha_close_surges_k<<<1, 1, 0, reinterpret_cast<cudaStream_t>(stream)>>>();
+  HA_CK(cudaGetLastError());
+  return HA_OK;
+}
+
 extern "C" int ha_trim_c(uint64_t max_bytes, void *stream, uint64_t *released_bytes) {
   if (released_bytes) *released_bytes = 0;
   HostDev *h = current();
@@ -821,6 +850,8 @@ extern "C" int ha_trim_c(uint64_t max_bytes, void *stream, uint64_t *released_by
                               cudaMemcpyHostToDevice, s) != cudaSuccess)
     rc = HA_ECUDA;
   if (rc == HA_OK) {
+    // surge heads hold slabs that would otherwise be wholly free
+    ha_close_surges_k<<<1, 1, 0, s>>>();
     ha_trim_k<<<(ncand + 127) / 128, 128, 0, s>>>(ncand, max_slabs);
     if (cudaGetLastError() != cudaSuccess ||
         cudaMemcpyFromSymbolAsync(&n, ha::g_trim_n, sizeof(n), 0, cudaMemcpyDeviceToHost, s) !=

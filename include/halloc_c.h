@@ -178,6 +178,15 @@ int ha_set_heads_c(uint32_t nheads);
    reference (halloc src/slab.cuh:378-445 has one head per size). */
 int ha_set_surge_c(int on);
 
+/* Closes every size's surge head sets now, on `stream`: their heads and
+   prefetched slabs are filed by occupancy (empty ones to the free set), and
+   each size is back to its single head until the next storm.  Open sets
+   otherwise close one level per calm head change, or all at once when a
+   size runs short of slabs; a program that has gone quiet can call this
+   (ha_trim_c does) to see every empty slab in the free set.  Run it while
+   no kernel allocates.  No counterpart in the reference. */
+int ha_close_surges_c(void *stream);
+
 /* Test hook for failure detection: sets the head-replacement lock of size
    class `size_id` to `held` (1 = held by a holder that never releases it,
    0 = free).  A hamalloc that then needs a new head for that size waits

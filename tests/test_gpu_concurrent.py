@@ -145,7 +145,16 @@ def test_freed_slabs_are_reused_across_sizes(torch_cuda):
             H.free_batch(ptrs, n, 1)
             torch.cuda.synchronize()
         assert_empty(H)
+        # every slab is in the free set or serves as a head or prefetched
+        # slab (surge sets of the sizes that stormed may still hold some);
+        # closing the surge sets leaves at most the head and prefetched slab
+        # of each size
+        end = H.stats()
+        assert end["free_slabs"] + end["head_slabs"] == st["nsbs"]
+        H.close_surges()
+        torch.cuda.synchronize()
         assert H.stats()["free_slabs"] >= st["nsbs"] - 2 * 16
+        assert H.stats()["surge_level"] == [0] * 16
         assert H.status() == 0
 
 
