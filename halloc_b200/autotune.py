@@ -2,8 +2,8 @@
 
 Sweeps, in three stages, the slab size {2, 4, 8} MiB x busy fraction
 {0.745, 0.835, 0.91} (sparse fraction follows: 0.012 or 0.0125); then, at the
-best of those, the request-group size (threads per persistent block: 4, 8 or
-16 warps) x the probe hash-step scale {50, 100, 200} %; then the head slabs
+best of those, the request-group size (threads per persistent block: 4, 8, 16
+or 32 warps) x the probe hash-step scale {50, 100, 200} %; then the head slabs
 per size {1, 2, 4}.  Each point re-initialises the allocator, prepares the
 graph-captured persistent launch and keeps the best of `reps` timed
 replays.  Only settings with hash scale 100 and one head keep the
@@ -51,7 +51,7 @@ def _time_point(torch, runner: BatchedRunner, opts: HallocOpts, block: int, item
 
 SLAB_SHIFTS = (21, 22, 23)          # 2, 4, 8 MiB slabs
 BUSY_FRACTIONS = (0.745, 0.835, 0.91)
-BLOCKS = (128, 256, 512)             # threads per persistent block: 4, 8, 16 warps
+BLOCKS = (128, 256, 512, 1024)       # threads per persistent block: 4 to 32 warps
 HASH_PCTS = (50, 100, 200)
 HEADS = (2, 4)
 

@@ -611,7 +611,8 @@ struct NoAllocOffsets {
   uint32_t free_start[kNoAllocMaxBatches + 2];
 };
 
-// Builds the task table of ha_batched_prepare_c in the scratch array and
+// Builds the task table of ha_batched_prepare_c (the same order: each step's
+// allocation chunks, then its free chunks) in the scratch array and
 // clears the queue and completion counters.  The host has checked that the
 // offsets never decrease and that the table has at most kNoAllocMaxTasks
 // entries; indices are 64-bit and the writes stop at the limit regardless.
@@ -623,17 +624,18 @@ __global__ void ha_noalloc_tasks_k(unsigned char *scratch, uint32_t nbatch, uint
   unsigned int *ctl = reinterpret_cast<unsigned int *>(scratch + kNaCtlOff);
   uint32_t n = 0;
   for (uint32_t st = 0; st <= nbatch; st++) {
+    ctl[1 + st] = 0;
+    if (st < nbatch) {
+      btasks[st] = 0;
+      const uint64_t b1 = off.batch_start[st + 1];
+      for (uint64_t r = off.batch_start[st]; r < b1 && n < kNoAllocMaxTasks; r += items) {
+        tasks[n++] = {(uint32_t)r, (uint32_t)(r + items < b1 ? r + items : b1), st, 0u};
+        btasks[st]++;
+      }
+    }
     const uint64_t f1 = off.free_start[st + 1];
     for (uint64_t k = off.free_start[st]; k < f1 && n < kNoAllocMaxTasks; k += items)
       tasks[n++] = {(uint32_t)k, (uint32_t)(k + items < f1 ? k + items : f1), st, 1u};
-    ctl[1 + st] = 0;
-    if (st == nbatch) break;
-    btasks[st] = 0;
-    const uint64_t b1 = off.batch_start[st + 1];
-    for (uint64_t r = off.batch_start[st]; r < b1 && n < kNoAllocMaxTasks; r += items) {
-      tasks[n++] = {(uint32_t)r, (uint32_t)(r + items < b1 ? r + items : b1), st, 0u};
-      btasks[st]++;
-    }
   }
   ctl[0] = 0;
 }
@@ -1205,20 +1207,25 @@ extern "C" int ha_batched_prepare_c(const ha_batch_plan_t *plan, uint32_t block,
   uint64_t ntasks = 0;
   if (check_plan_offsets(plan, task_items, &ntasks) != HA_OK || ntasks > 0xffffffffull)
     return HA_EINVAL;
-  // task table: for each step its free chunks, then its allocation chunks
+  // task table: for each step its allocation chunks, then its free chunks.
+  // A free chunk of step s waits for every batch before s; queued after
+  // batch s's allocations it is taken when batch s - 1 has long been taken
+  // (and has most likely finished), so blocks seldom idle at a step.
   std::vector<BatchTask> tasks;
   std::vector<uint32_t> btasks(plan->nbatch + 1, 0);
   tasks.reserve((size_t)ntasks);
   for (uint32_t st = 0; st <= plan->nbatch; st++) {
+    if (st < plan->nbatch) {
+      const uint64_t b1 = plan->h_batch_start[st + 1];
+      for (uint64_t r = plan->h_batch_start[st]; r < b1; r += task_items) {
+        tasks.push_back({(uint32_t)r, (uint32_t)(r + task_items < b1 ? r + task_items : b1), st,
+                         0u});
+        btasks[st]++;
+      }
+    }
     const uint64_t f1 = plan->h_free_start[st + 1];
     for (uint64_t k = plan->h_free_start[st]; k < f1; k += task_items)
       tasks.push_back({(uint32_t)k, (uint32_t)(k + task_items < f1 ? k + task_items : f1), st, 1u});
-    if (st == plan->nbatch) break;
-    const uint64_t b1 = plan->h_batch_start[st + 1];
-    for (uint64_t r = plan->h_batch_start[st]; r < b1; r += task_items) {
-      tasks.push_back({(uint32_t)r, (uint32_t)(r + task_items < b1 ? r + task_items : b1), st, 0u});
-      btasks[st]++;
-    }
   }
   int dev = 0, nsm = 0, fit = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||

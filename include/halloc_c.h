@@ -412,9 +412,9 @@ typedef struct ha_batch_plan_t {
 int ha_batched_plain_c(const ha_batch_plan_t *plan, uint32_t block, void *stream);
 
 /* Persistent form: ONE kernel whose resident blocks take tasks (chunks of
-   task_items requests) from a queue in step order; a free task waits
-   (bounded) until every allocation task of the earlier batches has
-   finished.  `block` threads per block ("request group"), ctas_per_sm
+   task_items requests) from a queue in step order, each step's allocation
+   chunks before its free chunks; a free task waits (bounded) until every
+   allocation task of the earlier batches has finished.  `block` threads per block ("request group"), ctas_per_sm
    blocks per SM (0 = as many as fit).  use_graph != 0 captures
    [clear acc, reset queue, kernel] in a CUDA graph once, replayed by each
    ha_batched_launch_c.  Returns an opaque handle in *out. */
