@@ -118,6 +118,26 @@ __device__ __forceinline__ void throughput_thread(uint32_t i, uint32_t sz, uint3
                                                   uint32_t niters, unsigned long long &sum,
                                                   unsigned long long &nfail) {
   const uint4 word = make_uint4(i ^ 0u, i ^ 1u, i ^ 2u, i ^ 3u);
+  if (nallocs == 1) {
+    // one block per iteration (the plain configuration): the same steps
+    // with the pointer in a register rather than the local array below
+    for (uint32_t it = 0; it < niters; it++) {
+      void *p = kCudaHeap ? malloc(sz) : hamalloc(sz);
+      if (!p) {
+        nfail++;
+        continue;
+      }
+      store16(p, word);
+      const uint4 v = load16(p);
+      HA_STAMP(ha::kStUser, v.x);
+      sum += (unsigned long long)v.x + v.y + v.z + v.w;
+      if (kCudaHeap)
+        free(p);
+      else
+        hafree(p);
+    }
+    return;
+  }
   void *ps[kMaxAllocsPerThread];
   for (uint32_t it = 0; it < niters; it++) {
     for (uint32_t a = 0; a < nallocs; a++) {
