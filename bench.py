@@ -748,6 +748,9 @@ def run_halloc_programs() -> dict:
 
 
 BATCH_POOL, BATCH_HF = 4 << 30, 0.5
+# launch shape of the persistent form: 32 warps per block, 8,192 requests per
+# task (the fastest of a 3 x 3 x 3 sweep of block, task size and blocks per SM)
+PERSIST_BLOCK, PERSIST_ITEMS = 1024, 8192
 
 
 def run_batched(torch, H, reps: int, tune: bool) -> dict:
@@ -780,7 +783,7 @@ def run_batched(torch, H, reps: int, tune: bool) -> dict:
 
     plain = timed(lambda: runner.plain(block=256, stream=stream))
     try:
-        h = runner.prepare(block=256, task_items=2048, graph=True)
+        h = runner.prepare(block=PERSIST_BLOCK, task_items=PERSIST_ITEMS, graph=True)
         pers = timed(lambda: runner.launch(h, stream))
     except Exception as e:  # report the plain form even so
         runner.release()
@@ -796,7 +799,7 @@ def run_batched(torch, H, reps: int, tune: bool) -> dict:
                      "launches": int(np.count_nonzero(np.diff(plan.free_start))) +
                      int(np.count_nonzero(np.diff(plan.batch_start)))},
            "persistent_graph": {"value": n / (min(pers) * 1e-3), "ms": pers, "launches": 1,
-                                "block": 256, "task_items": 2048},
+                                "block": PERSIST_BLOCK, "task_items": PERSIST_ITEMS},
            "speedup": min(plain) / min(pers), "ok": ok,
            "pool": {"memory": BATCH_POOL, "halloc_fraction": BATCH_HF}}
     if tune:
@@ -836,7 +839,7 @@ def run_batched_small_only(torch, H, reps: int, tune: bool = False) -> dict:
                 runner.verify()
                 ms.append(e0.elapsed_time(e1))
             out[name] = {"value": plan.nreq / (min(ms) * 1e-3), "ms": ms}
-        h = runner.prepare(block=256, task_items=2048, graph=True)
+        h = runner.prepare(block=PERSIST_BLOCK, task_items=PERSIST_ITEMS, graph=True)
         runner.launch(h, stream)
         torch.cuda.synchronize()
         runner.verify()

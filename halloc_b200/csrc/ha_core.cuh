@@ -291,9 +291,15 @@ __device__ __forceinline__ uint32_t *set_sums(uint32_t k) { return g_st.sums[k];
 // between: a tidy that clears a summary bit set by a concurrent put is
 // ordered after that put's word write and therefore sees it and restores
 // the bit.  Summary bits may be stale-set (harmless), never stale-clear.
+// The free set also keeps a count of its slabs (g_st.n_free).
 __device__ __forceinline__ void set_put(uint32_t k, uint32_t sb) {
   uint32_t w = sb >> 5;
-  red_or(&set_words(k)[w], 1u << (sb & 31));
+  if (k == kSetFree) {
+    if (!(atom_or(&set_words(k)[w], 1u << (sb & 31)) & (1u << (sb & 31))))
+      red_add(&g_st.n_free, 1u);
+  } else {
+    red_or(&set_words(k)[w], 1u << (sb & 31));
+  }
   fence_acq_rel();
   red_or(&set_sums(k)[w >> 5], 1u << (w & 31));
   red_add(&g_st.set_epoch, 1u);
@@ -315,6 +321,7 @@ __device__ __forceinline__ bool set_claim(uint32_t k, uint32_t sb) {
   uint32_t w = sb >> 5, bit = 1u << (sb & 31);
   uint32_t old = atom_and(&set_words(k)[w], ~bit);
   if (!(old & bit)) return false;
+  if (k == kSetFree) red_add(&g_st.n_free, 0u - 1u);
   if ((old & ~bit) == 0) set_tidy(k, w);
   return true;
 }
@@ -332,6 +339,7 @@ __device__ __noinline__ uint32_t set_take(uint32_t k) {
         uint32_t b = __ffs(word) - 1, bit = 1u << b;
         uint32_t old = atom_and(&words[w], ~bit);
         if (old & bit) {
+          if (k == kSetFree) red_add(&g_st.n_free, 0u - 1u);
           if ((old & ~bit) == 0) set_tidy(k, w);
           return w * 32 + b;
         }
@@ -737,9 +745,13 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
       const uint32_t per_set = storm >> level;
       const bool crowded = per_set >= kSurgeQueueMin && tickets < kSurgeTicketsUp * per_set;
       const bool calm = per_set < kSurgeQueueMin / 4 || tickets >= kSurgeTicketsDown * per_set;
-      if ((storm >= kSurgeUp || crowded) && level < kMaxLevel)
+      // more heads hold more partly filled slabs: open a level only while a
+      // quarter of the pool is free, and close one when under an eighth is
+      const uint32_t nfree = ld_relaxed(&g_st.n_free);
+      const uint32_t committed = ld_relaxed(&g_st.committed);
+      if ((storm >= kSurgeUp || crowded) && level < kMaxLevel && 4ull * nfree >= committed)
         nlevel = level + 1;
-      else if (storm < kSurgeDown && calm && level > 0)
+      else if (level > 0 && ((storm < kSurgeDown && calm) || 8ull * nfree < committed))
         nlevel = level - 1;
     }
     st_release(head, head_word(next, nlevel));

@@ -121,6 +121,7 @@ struct State {
   uint32_t n_null;
   uint32_t committed;     // slabs backed by device memory
   uint32_t n_surge_changes;  // surge level changes since init
+  uint32_t n_free;        // slabs in the free set
   // bumped by every insertion into a slab set; no_slab[hs] = epoch + 1 when
   // the last head search for (head, size) hs found nothing at that epoch
   alignas(128) uint32_t set_epoch;

@@ -461,6 +461,7 @@ int init_impl(const ha_opts_c &o) {
     }
     st->wait_limit_us = ha::kDefaultWaitUs;
     st->committed = committed;
+    st->n_free = committed;  // every backed slab starts in the free set
     for (uint32_t sb = 0; sb < nsbs; sb++) {
       st->ctr[sb * ha::kCtrStride] = ha::kCtrInit;
       st->desc[sb].size_id = ha::kNone;

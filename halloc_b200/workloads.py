@@ -102,7 +102,7 @@ class BatchedRunner:
         _check(self.lib.ha_batched_plain_c(ctypes.byref(self.c), block, _stream(stream)),
                "ha_batched_plain_c")
 
-    def prepare(self, block: int = 256, ctas_per_sm: int = 0, task_items: int = 2048,
+    def prepare(self, block: int = 1024, ctas_per_sm: int = 0, task_items: int = 8192,
                 graph: bool = True):
         h = ctypes.c_void_p()
         _check(self.lib.ha_batched_prepare_c(ctypes.byref(self.c), block, ctas_per_sm,

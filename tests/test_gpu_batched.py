@@ -63,7 +63,7 @@ r = BatchedRunner(plan, torch)
 r.plain(block=256)
 torch.cuda.synchronize()
 plain = r.acc()
-h = r.prepare(block=256, task_items=2048, graph=True)
+h = r.prepare(block=1024, task_items=8192, graph=True)
 r.launch(h)
 torch.cuda.synchronize()
 persistent = r.acc()
