@@ -163,13 +163,15 @@ int ha_set_heads_c(uint32_t nheads);
 
 /* Surge head sets (on by default with one head per size; applied by the
    next init on this process).  When thousands of warps queue for one size's
-   head replacement during one head's life (kSurgeUp = 2,048 queued warps: a
-   grid of 1,024 warps can never get there), the size gets 2, then 4, then
-   8 head slabs, each serving the SMs whose id modulo the set count names
-   it; the sets close again one level per head change that saw fewer than
-   256 queued warps, and all of them at once when the size runs short of
-   slabs, so a NULL still means that no slab is left for the size.  A thread
-   alone, or any grid that never queues that many warps, keeps the
+   head replacement during one head's life (2,048 queued warps: a grid of
+   1,024 warps can never get there), or when a long queue forms at a head
+   that serves only a few allocations per queued warp (under 96), the size
+   gets 2, then 4, then 8 head slabs, each serving the SMs whose id modulo
+   the set count names it -- while a quarter of the pool's slabs is free.
+   The sets close again one level per calm head change (or while under an
+   eighth of the pool is free), and all of them at once when a size runs
+   short of slabs, so a NULL still means that no slab is left for the size.
+   A thread alone, or any grid that never queues that many warps, keeps the
    reference policy's single head and addresses.  0 turns them off (the
    reference policy under every load), 1 on, -1 back to the environment's
    choice; HALLOC_SURGE=0|1 in the environment does the same for programs
