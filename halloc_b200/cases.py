@@ -1,7 +1,7 @@
 """Small instances of the workload kernels, each launched once, for
 profiling one kernel at a time and as short usage examples:
 
-    python -m halloc_b200.cases phase_ref|phase|batched|graph|samples|storm|serve|all
+    python -m halloc_b200.cases phase_ref|phase|batched|batched_small|graph|samples|storm|serve|all
 
 Every case holds at most about 1.1 GB on the device and checks its
 result the way the tests do (counts, checksums, an empty pool at the end);
@@ -89,6 +89,27 @@ def batched(torch) -> None:
     _done("batched")
 
 
+def batched_small(torch) -> None:
+    """The batched stream without its large requests: 16 batches of
+    1,024..262,144 requests, sizes geometric over the 16 classes; per-batch
+    launches, then one persistent launch with the benchmark's launch shape
+    (1,024 threads, 8,192 requests per task)."""
+    from halloc_b200.workloads import BatchedRunner, batched_plan
+    plan = batched_plan(seed=3, nbatch=16, max_batch=1 << 18, large_frac=0.0)
+    runner = BatchedRunner(plan, torch)
+    H.init(H.HallocOpts(memory=1 << 30, halloc_fraction=0.5))
+    stream = torch.cuda.current_stream()
+    runner.plain(block=256, stream=stream)
+    torch.cuda.synchronize()
+    runner.verify()
+    h = runner.prepare(block=1024, task_items=8192, graph=False)
+    runner.launch(h, stream)
+    torch.cuda.synchronize()
+    runner.verify()
+    runner.release()
+    _done("batched_small")
+
+
 def graph(torch) -> None:
     """Random graph of 262,144 vertices, Poisson(16) out-degree, doubling
     neighbour arrays: ha_graph_build_k, then the CSR gather."""
@@ -172,7 +193,8 @@ def serve(torch) -> None:
     _done("serve")
 
 
-CASES = {"phase_ref": phase_ref, "phase": phase, "batched": batched, "graph": graph,
+CASES = {"phase_ref": phase_ref, "phase": phase, "batched": batched,
+         "batched_small": batched_small, "graph": graph,
          "samples": samples, "storm": storm, "serve": serve}
 
 
