@@ -548,33 +548,32 @@ __device__ __forceinline__ uint64_t now_ns() {
 }
 
 // Persistent form.  ctl[0] = next task; ctl[1 + b] = finished allocation
-// tasks of batch b; btasks[b] = allocation tasks of batch b.  Each warp takes
-// tasks of its own (a task is task_items requests, one per lane in turn), so
-// no lane waits at a block barrier for the slowest allocation of another
-// warp.  A free task of step s starts once every batch b < s is complete;
-// each warp remembers the batches it has already seen complete (tasks reach
-// a warp in step order).
+// tasks of batch b; btasks[b] = allocation tasks of batch b.  A free task of
+// step s starts once every batch b < s is complete; each block remembers the
+// batches it has already seen complete (tasks reach a block in step order).
 __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uint32_t *btasks,
                               const uint32_t *req_size, unsigned long long *req_ptr,
                               const uint32_t *free_ids, unsigned int *ctl,
                               unsigned long long *acc) {
-  const uint32_t lane = threadIdx.x & 31u;
+  __shared__ uint32_t s_task, s_done_below;
   unsigned long long nfail = 0, nmal = 0, bad = 0, idsum = 0, nfree = 0, late = 0;
-  uint32_t done_below = 0;  // lane 0: batches below this are complete
+  if (threadIdx.x == 0) s_done_below = 0;
   for (;;) {
-    uint32_t t = 0;
-    if (lane == 0) t = atomicAdd(&ctl[0], 1u);
-    t = __shfl_sync(0xffffffffu, t, 0);
+    __syncthreads();  // everyone has read s_task
+    if (threadIdx.x == 0) s_task = atomicAdd(&ctl[0], 1u);
+    __syncthreads();
+    const uint32_t t = s_task;
     if (t >= ntasks) break;
     const BatchTask tk = tasks[t];
     if (tk.is_free) {
-      if (lane == 0) {
-        // every allocation task of those batches was taken earlier by a
-        // running warp, so each wait ends
+      if (threadIdx.x == 0) {
+        // every allocation task of those batches was dequeued earlier by a
+        // running block, so each wait ends
         const uint64_t limit = now_ns() + 2000000000ull;
-        while (done_below < tk.step) {
-          if (ld_acquire_u32(&ctl[1 + done_below]) >= btasks[done_below]) {
-            done_below++;
+        uint32_t b = s_done_below;
+        while (b < tk.step) {
+          if (ld_acquire_u32(&ctl[1 + b]) >= btasks[b]) {
+            b++;
             continue;
           }
           if (now_ns() > limit) {
@@ -583,16 +582,17 @@ __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uin
           }
           __nanosleep(128);
         }
+        s_done_below = b;
       }
-      __syncwarp();  // the other lanes read what those batches wrote
-      for (uint32_t k = tk.begin + lane; k < tk.end; k += 32)
+      __syncthreads();
+      for (uint32_t k = tk.begin + threadIdx.x; k < tk.end; k += blockDim.x)
         batched_free_one(k, free_ids, req_ptr, bad, idsum, nfree);
     } else {
-      for (uint32_t r = tk.begin + lane; r < tk.end; r += 32)
+      for (uint32_t r = tk.begin + threadIdx.x; r < tk.end; r += blockDim.x)
         batched_malloc_one(r, req_size, req_ptr, nfail, nmal);
-      __syncwarp();  // the warp's req_ptr and payload writes, then the count
-      if (lane == 0) {
-        __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();  // this block's req_ptr and payload writes before the count
         atomicAdd(&ctl[1 + tk.step], 1u);
       }
     }
