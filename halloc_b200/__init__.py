@@ -80,7 +80,7 @@ class _CStats(ctypes.Structure):
                 ("cached", ctypes.c_uint32 * 16), ("growth", ctypes.c_uint32),
                 ("committed_slabs", ctypes.c_uint32), ("unit_bytes", ctypes.c_uint64),
                 ("surge_level", ctypes.c_uint32 * 16), ("n_surge_changes", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("free_count", ctypes.c_uint32)]
 
 
 class _CPhaseResult(ctypes.Structure):
@@ -256,7 +256,7 @@ def stats() -> dict:
     s = _CStats()
     _check(load().ha_stats_c(ctypes.byref(s)), "ha_stats_c")
     arrays = ("head", "cached", "surge_level")
-    d = {f: getattr(s, f) for f, _ in _CStats._fields_ if f not in arrays + ("reserved",)}
+    d = {f: getattr(s, f) for f, _ in _CStats._fields_ if f not in arrays}
     for f in arrays:
         d[f] = list(getattr(s, f))
     return d

@@ -743,7 +743,7 @@ extern "C" int ha_stats_c(ha_stats_t *out) {
   ha::StatsOut s;
   int rc = run_stats(0, &s);
   if (rc) return rc;
-  uint32_t head[ha::kNSizes], cached[ha::kNSizes], misc[6];
+  uint32_t head[ha::kNSizes], cached[ha::kNSizes], misc[7];
   HA_CK(cudaMemcpyFromSymbol(head, ha::g_st, sizeof(head), offsetof(ha::State, head)));
   HA_CK(cudaMemcpyFromSymbol(cached, ha::g_st, sizeof(cached), offsetof(ha::State, cached)));
   HA_CK(cudaMemcpyFromSymbol(misc, ha::g_st, sizeof(misc), offsetof(ha::State, status)));
@@ -767,6 +767,7 @@ extern "C" int ha_stats_c(ha_stats_t *out) {
   }
   memcpy(out->cached, cached, sizeof(cached));
   out->n_surge_changes = misc[5];
+  out->free_count = misc[6];
   out->growth = h->growth ? 1 : 0;
   out->committed_slabs = misc[4];
   out->unit_bytes = h->unit_bytes;

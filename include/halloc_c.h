@@ -85,7 +85,9 @@ typedef struct ha_stats_t {
   uint64_t unit_bytes;      /* growth / release unit, a multiple of the slab size */
   uint32_t surge_level[16]; /* per size class: 2^level head sets open (0 = one) */
   uint32_t n_surge_changes; /* surge level changes since init */
-  uint32_t reserved;
+  uint32_t free_count;      /* the free set's own count of its slabs (kept by
+                               its operations; equals free_slabs when no
+                               kernel runs) */
 } ha_stats_t;
 
 /* Fills *out (synchronises the device).  No counterpart in the reference,

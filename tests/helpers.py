@@ -192,3 +192,12 @@ def allocator(**opts):
         yield H
     finally:
         H.shutdown()
+
+
+def assert_free_count(H) -> dict:
+    """The free set's own count of its slabs (kept by the set operations)
+    equals the slabs its bits hold, counted by the statistics kernel: to be
+    called when no kernel runs."""
+    st = H.stats()
+    assert st["free_count"] == st["free_slabs"], (st["free_count"], st["free_slabs"])
+    return st

@@ -7,7 +7,7 @@ derives from the live blocks."""
 import numpy as np
 import pytest
 
-from tests.helpers import (allocator, check_blocks, expected_slab_state,
+from tests.helpers import (allocator, assert_free_count, check_blocks, expected_slab_state,
                            nibbles_to_chunk_layout, plain_checksum)
 
 pytestmark = pytest.mark.gpu
@@ -149,11 +149,11 @@ def test_freed_slabs_are_reused_across_sizes(torch_cuda):
         # slab (surge sets of the sizes that stormed may still hold some);
         # closing the surge sets leaves at most the head and prefetched slab
         # of each size
-        end = H.stats()
+        end = assert_free_count(H)
         assert end["free_slabs"] + end["head_slabs"] == st["nsbs"]
         H.close_surges()
         torch.cuda.synchronize()
-        assert H.stats()["free_slabs"] >= st["nsbs"] - 2 * 16
+        assert assert_free_count(H)["free_slabs"] >= st["nsbs"] - 2 * 16
         assert H.stats()["surge_level"] == [0] * 16
         assert H.status() == 0
 

@@ -7,7 +7,7 @@ payload intact across grows and trims."""
 import numpy as np
 import pytest
 
-from tests.helpers import check_blocks, expected_slab_state, plain_checksum
+from tests.helpers import assert_free_count, check_blocks, expected_slab_state, plain_checksum
 
 pytestmark = pytest.mark.gpu
 
@@ -110,11 +110,13 @@ def test_payload_through_grow_and_trim(torch_cuda, growing):
     assert released >= 1 << 30 and released % before["unit_bytes"] == 0
     assert after["committed_slabs"] == before["committed_slabs"] - released // before["sb_sz"]
     assert after["used_chunks"] == 0 and H.status() == 0
+    assert_free_count(H)
     assert loop(16, 32768) == [plain_checksum(32768, 12), 0]
     H.grow(256 * MiB)
     torch.cuda.synchronize()
     assert loop(512) == [plain_checksum(65536, 12), 0]
     assert H.stats()["used_chunks"] == 0 and H.status() == 0
+    assert_free_count(H)
 
 
 def test_trim_keeps_units_with_live_blocks(torch_cuda, growing):
@@ -148,6 +150,7 @@ def test_trim_keeps_units_with_live_blocks(torch_cuda, growing):
     H.strings_free(n, strs)
     torch.cuda.synchronize()
     assert H.stats()["used_chunks"] == 0 and H.status() == 0
+    assert_free_count(H)
 
 
 def test_grow_and_trim_need_growth_mode(torch_cuda):

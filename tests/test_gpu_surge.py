@@ -14,7 +14,7 @@ and show that a lone thread never opens one.
 import numpy as np
 import pytest
 
-from tests.helpers import allocator, check_blocks, plain_checksum
+from tests.helpers import allocator, assert_free_count, check_blocks, plain_checksum
 from tests.test_gpu_concurrent import assert_empty, assert_state_matches_live, malloc_batch
 
 pytestmark = pytest.mark.gpu
@@ -43,6 +43,11 @@ def test_storm_opens_surge_sets_and_stays_exact(torch_cuda, surge_default):
         st = H.stats()
         assert st["n_surge_changes"] > 0
         assert st["used_chunks"] == 0 and H.status() == 0
+        assert_free_count(H)
+        H.close_surges()
+        torch.cuda.synchronize()
+        st = assert_free_count(H)
+        assert st["surge_level"] == [0] * 16 and st["head_slabs"] <= 2 * 16
 
 
 def test_blocks_held_under_a_storm(torch_cuda, surge_default):
@@ -62,7 +67,7 @@ def test_blocks_held_under_a_storm(torch_cuda, surge_default):
         H.free_batch(ptrs, n, 1)
         torch.cuda.synchronize()
         assert_empty(H)
-        st = H.stats()
+        st = assert_free_count(H)
         assert st["free_slabs"] + st["head_slabs"] == st["nsbs"]
         assert H.status() == 0
 
@@ -108,6 +113,7 @@ def _exhaust(torch, H, surge: bool):
         H.free_batch(ptrs, n, 1)
         torch.cuda.synchronize()
         assert_empty(H)
+        assert_free_count(H)
         assert H.status() == 0
         return r["n"], changes
 
