@@ -561,7 +561,7 @@ ha_opts_c to_c(const halloc_opts_t &o) {
 __global__ void ha_adopt_k(uint32_t first, uint32_t count) {
   using namespace ha;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < count) set_put(kSetFree, first + i);
+  if (i < count) set_put_free(first + i);
   if (i == 0) red_add(&g_st.committed, count);
 }
 
@@ -617,7 +617,7 @@ __global__ void ha_trim_k(uint32_t ncand, uint32_t max_slabs) {
     }
     atomicSub(&g_trim_slabs, n);
   }
-  for (uint32_t k = 0; k < taken; k++) set_put(kSetFree, first + k);
+  for (uint32_t k = 0; k < taken; k++) set_put_free(first + k);
 }
 
 // ---- statistics kernels ----------------------------------------------------
