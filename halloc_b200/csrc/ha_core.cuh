@@ -57,21 +57,6 @@ __device__ __forceinline__ uint32_t sm_id() {
   asm("mov.u32 %0, %%smid;" : "=r"(v));
   return v;
 }
-__device__ __forceinline__ uint32_t clock_lo() {
-  uint32_t c;
-  asm volatile("mov.u32 %0, %%clock;" : "=r"(c));
-  return c;
-}
-// The SM clock, read once `dep` (a value a load or atomic returned) is
-// available: the read is predicated on it.
-__device__ __forceinline__ uint32_t clock_after(uint32_t dep) {
-  uint32_t c;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0x5bd1e995;\n\t"
-      "@p mov.u32 %0, %%clock;\n\t@!p mov.u32 %0, %%clock;\n\t}"
-      : "=r"(c) : "r"(dep) : "memory");
-  return c;
-}
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -314,7 +299,10 @@ __device__ __forceinline__ void set_put(uint32_t k, uint32_t sb) {
   red_add(&g_st.set_epoch, 1u);
 }
 // Files slab sb into the free set, which keeps a count of its slabs
-// (g_st.n_free; taken slabs are counted off by set_take / set_claim).
+// (g_st.n_free; taken slabs are counted off by set_take / set_claim), for
+// slabs that may be in it already.  The allocator's own paths file only
+// slabs that are not, with set_put and an increment of the count: a call
+// here from them costs every hamalloc a larger register frame.
 __device__ __noinline__ void set_put_free(uint32_t sb) {
   const uint32_t w = sb >> 5, bit = 1u << (sb & 31);
   if (!(atom_or(&set_words(kSetFree)[w], bit) & bit)) red_add(&g_st.n_free, 1u);
@@ -387,7 +375,8 @@ __device__ __noinline__ void try_release(uint32_t sb, uint32_t cid, bool from_he
       st_relaxed(&d->size_id, kNone);
       st_relaxed(&d->chunk_id, kNone);
       st_relaxed(&d->chunk_enc, 0);
-      set_put_free(sb);
+      set_put(kSetFree, sb);  // a slab in use until now: a new member
+      red_add(&g_st.n_free, 1u);
       fence_acq_rel();
       if (!from_head) set_drop(kSetSparse + cid, sb);
       return;
@@ -569,7 +558,8 @@ __device__ __noinline__ uint32_t find_slab(uint32_t sid) {
   }
   while ((sb = set_take(kSetFree)) != kNone) {
     if (!lock(&g_st.sb_lock[sb])) {
-      set_put_free(sb);
+      set_put(kSetFree, sb);  // taken (and counted off) just above
+      red_add(&g_st.n_free, 1u);
       return kNone;
     }
     Desc *d = &g_st.desc[sb];
@@ -644,30 +634,6 @@ __device__ __noinline__ bool close_other_surges(uint32_t own) {
     any = true;
   }
   return any;
-}
-
-// Opens one more surge level for size sid without a head change (the third
-// trigger): only if its set-0 lock is free at once, the level below the
-// maximum and a quarter of the pool free.  Clears the slow-commit count.
-__device__ __noinline__ void raise_level(uint32_t sid) {
-  uint32_t *hlock0 = &g_st.head_lock[sid * kTicketStride];
-  if (ld_relaxed(hlock0) != 0 || !try_lock(hlock0)) return;
-  const uint32_t w = ld_relaxed(&g_st.head[sid]);
-  const uint32_t nfree = ld_relaxed(&g_st.n_free);
-  const uint32_t committed = ld_relaxed(&g_st.committed);
-  const uint32_t level = head_level(w);
-  if (level < kMaxLevel && head_slab(w) != kNone && 4ull * nfree >= committed) {
-    st_release(&g_st.head[sid], head_word(head_slab(w), level + 1));
-    red_add(&g_st.n_surge_changes, 1);
-  }
-  st_relaxed(&g_st.storm[sid * kTicketStride + 2], 0);
-  unlock(hlock0);
-}
-
-// Counts a slow commit of size sid; true for the one that completes
-// kHotEvents (its caller raises the level, from the slow path).
-__device__ __forceinline__ bool note_hot(uint32_t sid) {
-  return atom_add(&g_st.storm[sid * kTicketStride + 2], 1u) == kHotEvents - 1;
 }
 
 // Hands a slab taken for head slot hs back to hs's prefetch slot, or, when
@@ -781,7 +747,6 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
       // grid: kSurgeTicketsUp each); close one when neither comes near.
       uint32_t *line = &g_st.storm[sid * kTicketStride];
       const uint32_t storm = atomicExch(line, 0u);
-      st_relaxed(line + 2, 0);  // slow commits count per head life
       const uint32_t tnow = ld_relaxed(&g_st.ticket[sid * kTicketStride]);
       const uint32_t tickets = tnow - ld_relaxed(line + 1);
       st_relaxed(line + 1, tnow);
@@ -938,23 +903,14 @@ __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t
 // Returns false, after undoing this lane's reservation, when the slab no
 // longer has the caller's chunk size; otherwise *crossed tells whether the
 // count crossed the busy threshold.
-// *hot is set for the group leader whose slow commit completes kHotEvents
-// (see note_hot).
 __device__ __forceinline__ bool commit(uint32_t rmask, uint32_t sb, uint32_t ncib,
                                        uint32_t cid, uint32_t busy, uint32_t pos,
-                                       uint32_t block, uint32_t sid, bool &crossed,
-                                       bool &hot) {
+                                       uint32_t block, bool &crossed) {
   const uint32_t grp = __match_any_sync(rmask, sb);
   const uint32_t total = __reduce_add_sync(grp, ncib);
   const uint32_t lead = __ffs(grp) - 1;
   uint32_t before = 0;
-  hot = false;
-  if (lane_id() == lead) {
-    const uint32_t t0 = clock_lo();
-    before = atom_add_meta(ctr_of(sb), total << kCntShift);
-    // a counter word queued behind thousands of warps (surge sets only)
-    if (c_cfg.surge && clock_after(before) - t0 > kHotCycles) hot = note_hot(sid);
-  }
+  if (lane_id() == lead) before = atom_add_meta(ctr_of(sb), total << kCntShift);
   before = __shfl_sync(grp, before, lead);
   const bool ok = ((before >> kChunkShift) & kChunkField) == cid;
   const uint32_t n0 = before >> kCntShift;
@@ -979,7 +935,6 @@ __device__ __forceinline__ void *publish(uint32_t sb, uint32_t pos, uint32_t enc
 constexpr uint32_t kWant = 1;      // no block yet
 constexpr uint32_t kNeedHead = 2;  // ask for a new head slab
 constexpr uint32_t kMidRound = 4;  // continue the current probe call at pos
-constexpr uint32_t kRaiseLevel = 8;  // open one more surge level (slow commits)
 
 // The rest of halloc's allocation loop (src/halloc.cu:145-179 with
 // src/slab.cuh:453-535), for the whole warp `warp`: new head slabs for the
@@ -997,7 +952,6 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
   const uint32_t first = first_probe(sid, ticket, c.ncib, mn, c.nchunks);
   const uint32_t block = (1u << c.ncib) - 1u;
   bool want = flags & kWant, need_head = flags & kNeedHead, mid = flags & kMidRound;
-  if (flags & kRaiseLevel) raise_level(sid);
   uint32_t rounds = 0;
   for (;;) {
     // -- new head slabs -------------------------------------------------------
@@ -1040,10 +994,8 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
       mid = false;
       const uint32_t rmask = __ballot_sync(want_mask, reserved);
       if (reserved) {
-        bool crossed, hot;
-        const bool ok = commit(rmask, sb, c.ncib, c.chunk_id, c.busy, pos, block, sid, crossed, hot);
-        if (hot) raise_level(sid);
-        if (ok) {
+        bool crossed;
+        if (commit(rmask, sb, c.ncib, c.chunk_id, c.busy, pos, block, crossed)) {
           if (crossed) need_head = true;
           p = publish(sb, pos, c.chunk_enc, c.ncib);
           want = false;
@@ -1128,15 +1080,14 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
   void *p = nullptr;
   const uint32_t rmask = __ballot_sync(warp, reserved);
   if (reserved) {
-    bool crossed, hot;
-    if (commit(rmask, sb, ncib, cid, __ldg(&g_cls[sid].busy), pos, block, sid, crossed, hot)) {
+    bool crossed;
+    if (commit(rmask, sb, ncib, cid, __ldg(&g_cls[sid].busy), pos, block, crossed)) {
       HA_STAMP(kStMallocCount, crossed);
       p = publish(sb, pos, enc, ncib);
       flags = crossed ? kNeedHead : 0;
     } else {
       flags = kWant | kNeedHead;
     }
-    if (hot) flags |= kRaiseLevel;
   }
   if (__any_sync(warp, flags != 0)) {
     HA_STAMP(kStSlowIn, flags);

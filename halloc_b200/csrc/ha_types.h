@@ -66,13 +66,6 @@ constexpr uint32_t kSurgeDown = 256;
 #ifndef HA_SURGE_TICKETS_UP
 #define HA_SURGE_TICKETS_UP 96  // 0 turns the second trigger off
 #endif
-// third trigger: kHotEvents commits of one size whose slab-counter atomic
-// took over kHotCycles SM cycles (a counter word queued behind thousands of
-// warps: a lone thread sees about 800, a 1,024-warp grid at most about 2,200)
-// within one set-0 head's life raise the level at once, for heads that never
-// fill and so never reach a head change
-constexpr uint32_t kHotCycles = 4000;
-constexpr uint32_t kHotEvents = 256;
 constexpr uint32_t kSurgeQueueMin = 128;
 constexpr uint32_t kSurgeTicketsUp = HA_SURGE_TICKETS_UP;
 constexpr uint32_t kSurgeTicketsDown = 4 * HA_SURGE_TICKETS_UP;
