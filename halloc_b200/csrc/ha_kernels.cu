@@ -336,18 +336,6 @@ __global__ void ha_phase_free_k(uint32_t n, uint32_t nslots, uint32_t seed, uint
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long filled = 0, rsum = 0, nfree = 0;
   if (i < n) {
-    // first the lines of every block this thread frees are fetched into L2
-    // at once, so that the read-backs below overlap instead of each waiting
-    // on DRAM in turn
-    for (uint32_t s = 0; s < nslots; s++) {
-      const size_t k = (size_t)s * n + i;
-      const char *p = static_cast<const char *>(slots[k]);
-      if (p && (thr == 0xffffffffu || slot_hash(seed, i, s, round) < thr)) {
-        const uintptr_t a = (uintptr_t)p, e = a + slot_sz[k];
-        for (uintptr_t l = a & ~(uintptr_t)127; l < e; l += 128)
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(l));
-      }
-    }
     for (uint32_t s = 0; s < nslots; s++) {
       const size_t k = (size_t)s * n + i;
       void *p = slots[k];
