@@ -38,7 +38,7 @@ PAIRS_PER_STEP = NTHREADS * NITERS * NALLOCS
 ATOMICS_PER_PAIR = 2  # one bit-array reservation + one release
 # DRAM bytes (read + write) of one launch of the plain kernel, from an ncu
 # capture of the current build (the bench cannot read DRAM counters itself)
-PLAIN_DRAM_BYTES_PER_LAUNCH = 186624
+PLAIN_DRAM_BYTES_PER_LAUNCH = 192000
 METRIC = "16B malloc/free pairs/s"
 WORKLOAD = ("plain: 256 x 128 threads, 10 x (hamalloc(16), 16-B write, read-back, hafree), "
             "512 MiB pool, default halloc_opts_t")
