@@ -757,9 +757,11 @@ __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
       // quarter of the pool is free, and close one when under an eighth is
       const uint32_t nfree = ld_relaxed(&g_st.n_free);
       const uint32_t committed = ld_relaxed(&g_st.committed);
-      if ((storm >= kSurgeUp || crowded) && level < kMaxLevel && 4ull * nfree >= committed)
+      if ((storm >= kSurgeUp || crowded) && level < kMaxLevel &&
+          (uint64_t)kSurgeFreeOpen * nfree >= committed)
         nlevel = level + 1;
-      else if (level > 0 && ((storm < kSurgeDown && calm) || 8ull * nfree < committed))
+      else if (level > 0 &&
+               ((storm < kSurgeDown && calm) || (uint64_t)kSurgeFreeClose * nfree < committed))
         nlevel = level - 1;
     }
     st_release(head, head_word(next, nlevel));

@@ -67,6 +67,16 @@ constexpr uint32_t kSurgeDown = 256;
 #define HA_SURGE_TICKETS_UP 96  // 0 turns the second trigger off
 #endif
 constexpr uint32_t kSurgeQueueMin = 128;
+// pool headroom: a level opens only while 1/kSurgeFreeOpen of the committed
+// slabs is free, and one closes per head change while under 1/kSurgeFreeClose
+#ifndef HA_SURGE_FREE_OPEN
+#define HA_SURGE_FREE_OPEN 4
+#endif
+#ifndef HA_SURGE_FREE_CLOSE
+#define HA_SURGE_FREE_CLOSE 8
+#endif
+constexpr uint32_t kSurgeFreeOpen = HA_SURGE_FREE_OPEN;
+constexpr uint32_t kSurgeFreeClose = HA_SURGE_FREE_CLOSE;
 constexpr uint32_t kSurgeTicketsUp = HA_SURGE_TICKETS_UP;
 constexpr uint32_t kSurgeTicketsDown = 4 * HA_SURGE_TICKETS_UP;
 
