@@ -165,3 +165,29 @@ def test_grow_and_trim_need_growth_mode(torch_cuda):
         assert H.stats()["committed_slabs"] == H.stats()["nsbs"]
     finally:
         H.shutdown()
+
+
+def test_trim_closes_surge_sets_first(torch_cuda, growing):
+    """A storm on a grown pool opens surge head sets; once everything is
+    freed, trim closes them before it looks for wholly free units, so the
+    memory their heads held goes back too: what stays backed is at most the
+    head and prefetched slab of each size, and the free set's count of its
+    slabs still matches its bits."""
+    torch, H = torch_cuda, growing
+    H.grow(1 << 30)
+    torch.cuda.synchronize()
+    n = 1 << 20
+    out = torch.zeros(2, dtype=torch.int64, device="cuda")
+    H.throughput(out, n, nbytes=256, block=256, nallocs=1, niters=2)
+    torch.cuda.synchronize()
+    assert out.cpu().tolist() == [plain_checksum(n, 2), 0]
+    st = assert_free_count(H)
+    assert st["n_surge_changes"] > 0 and st["used_chunks"] == 0
+    H.trim()
+    st = assert_free_count(H)
+    assert st["surge_level"] == [0] * 16
+    # every slab still backed is free or one of the single head / prefetched
+    # slab of a size
+    assert st["committed_slabs"] - st["free_slabs"] <= 2 * 16
+    assert st["head_slabs"] <= 2 * 16
+    assert H.status() & ~H.ST_GROW == 0
