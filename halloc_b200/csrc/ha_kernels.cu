@@ -547,6 +547,34 @@ __device__ __forceinline__ uint64_t now_ns() {
   return t;
 }
 
+// Within a block's task, warps take 32 consecutive requests at a time from a
+// shared-memory counter: a warp whose allocations were quick takes the next
+// 32, so the block's barrier at the end of the task waits for at most one
+// slow chunk rather than for the slowest of each thread's fixed share.
+// -DHA_BPERSIST_CHUNKS=0 gives every thread the fixed strided share instead.
+#ifndef HA_BPERSIST_CHUNKS
+#define HA_BPERSIST_CHUNKS 1
+#endif
+template <typename F>
+__device__ __forceinline__ void for_task_items(uint32_t begin, uint32_t end, uint32_t *next,
+                                               F &&f) {
+#if HA_BPERSIST_CHUNKS
+  // the block size is a multiple of 32 (checked by the host), so every warp
+  // is whole
+  const uint32_t lane = threadIdx.x & 31u, n = end - begin;
+  for (;;) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(next, 32u);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= n) break;
+    if (c + lane < n) f(begin + c + lane);
+  }
+#else
+  (void)next;
+  for (uint32_t r = begin + threadIdx.x; r < end; r += blockDim.x) f(r);
+#endif
+}
+
 // Persistent form.  ctl[0] = next task; ctl[1 + b] = finished allocation
 // tasks of batch b; btasks[b] = allocation tasks of batch b.  A free task of
 // step s starts once every batch b < s is complete; each block remembers the
@@ -555,12 +583,15 @@ __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uin
                               const uint32_t *req_size, unsigned long long *req_ptr,
                               const uint32_t *free_ids, unsigned int *ctl,
                               unsigned long long *acc) {
-  __shared__ uint32_t s_task, s_done_below;
+  __shared__ uint32_t s_task, s_done_below, s_next;
   unsigned long long nfail = 0, nmal = 0, bad = 0, idsum = 0, nfree = 0, late = 0;
   if (threadIdx.x == 0) s_done_below = 0;
   for (;;) {
-    __syncthreads();  // everyone has read s_task
-    if (threadIdx.x == 0) s_task = atomicAdd(&ctl[0], 1u);
+    __syncthreads();  // everyone has read s_task and is done with s_next
+    if (threadIdx.x == 0) {
+      s_task = atomicAdd(&ctl[0], 1u);
+      s_next = 0;
+    }
     __syncthreads();
     const uint32_t t = s_task;
     if (t >= ntasks) break;
@@ -585,11 +616,13 @@ __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uin
         s_done_below = b;
       }
       __syncthreads();
-      for (uint32_t k = tk.begin + threadIdx.x; k < tk.end; k += blockDim.x)
+      for_task_items(tk.begin, tk.end, &s_next, [&](uint32_t k) {
         batched_free_one(k, free_ids, req_ptr, bad, idsum, nfree);
+      });
     } else {
-      for (uint32_t r = tk.begin + threadIdx.x; r < tk.end; r += blockDim.x)
+      for_task_items(tk.begin, tk.end, &s_next, [&](uint32_t r) {
         batched_malloc_one(r, req_size, req_ptr, nfail, nmal);
+      });
       __syncthreads();
       if (threadIdx.x == 0) {
         __threadfence();  // this block's req_ptr and payload writes before the count
