@@ -498,12 +498,10 @@ __device__ __forceinline__ void batched_malloc_one(uint32_t r, const uint32_t *r
   }
 }
 
-__device__ __forceinline__ void batched_free_one(uint32_t k, const uint32_t *free_ids,
-                                                 unsigned long long *req_ptr,
+__device__ __forceinline__ void batched_free_req(uint32_t r, unsigned long long *req_ptr,
                                                  unsigned long long &bad,
                                                  unsigned long long &idsum,
                                                  unsigned long long &nfree) {
-  const uint32_t r = free_ids[k];
   void *p = (void *)(uintptr_t)req_ptr[r];
   if (!p) return;
   if (*reinterpret_cast<const unsigned long long *>(p) != r) bad++;
@@ -511,6 +509,14 @@ __device__ __forceinline__ void batched_free_one(uint32_t k, const uint32_t *fre
   nfree++;
   hafree(p);
   req_ptr[r] = 0;  // a later run (graph replay) starts from all-NULL pointers
+}
+
+__device__ __forceinline__ void batched_free_one(uint32_t k, const uint32_t *free_ids,
+                                                 unsigned long long *req_ptr,
+                                                 unsigned long long &bad,
+                                                 unsigned long long &idsum,
+                                                 unsigned long long &nfree) {
+  batched_free_req(free_ids[k], req_ptr, bad, idsum, nfree);
 }
 
 __global__ void ha_bmalloc_k(uint32_t begin, uint32_t end, const uint32_t *req_size,
@@ -540,6 +546,9 @@ __device__ __forceinline__ uint32_t ld_acquire_u32(const unsigned int *p) {
   uint32_t v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(unsigned int *p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ uint64_t now_ns() {
   uint64_t t;
@@ -575,14 +584,27 @@ __device__ __forceinline__ void for_task_items(uint32_t begin, uint32_t end, uin
 #endif
 }
 
+// A free task of step s frees blocks of batches before s.  Those of batches
+// before s - 1 were allocated long before (the block waits for them, which
+// seldom takes long); each block of batch s - 1 waits only for the
+// allocation task that made it, so a free task need not wait for the whole
+// of the batch just before it.  -DHA_BPERSIST_ITEM_WAIT=0 makes every free
+// task wait for all of batch s - 1 instead.
+#ifndef HA_BPERSIST_ITEM_WAIT
+#define HA_BPERSIST_ITEM_WAIT 1
+#endif
+
 // Persistent form.  ctl[0] = next task; ctl[1 + b] = finished allocation
-// tasks of batch b; btasks[b] = allocation tasks of batch b.  A free task of
-// step s starts once every batch b < s is complete; each block remembers the
-// batches it has already seen complete (tasks reach a block in step order).
+// tasks of batch b; btasks[b] = allocation tasks of batch b; bdep[b] = (first
+// request, first task index) of batch b; tdone[t] = 1 once allocation task t
+// is finished; `items` = requests per task (the last task of a batch may
+// hold fewer).  Each block remembers the batches it has already seen
+// complete (tasks reach a block in step order).
 __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uint32_t *btasks,
+                              const uint2 *bdep, uint32_t items,
                               const uint32_t *req_size, unsigned long long *req_ptr,
                               const uint32_t *free_ids, unsigned int *ctl,
-                              unsigned long long *acc) {
+                              unsigned int *tdone, unsigned long long *acc) {
   __shared__ uint32_t s_task, s_done_below, s_next;
   unsigned long long nfail = 0, nmal = 0, bad = 0, idsum = 0, nfree = 0, late = 0;
   if (threadIdx.x == 0) s_done_below = 0;
@@ -607,6 +629,7 @@ __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uin
             b++;
             continue;
           }
+          if (HA_BPERSIST_ITEM_WAIT && b + 1 == tk.step) break;  // per block, below
           if (now_ns() > limit) {
             late++;
             break;
@@ -616,8 +639,31 @@ __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uin
         s_done_below = b;
       }
       __syncthreads();
+      // blocks of batch step - 1, when it is not known to be complete: the
+      // allocation task of each is tasks dep_task .. dep_task + dep_n - 1
+      uint32_t dep_begin = 0xffffffffu, dep_task = 0, dep_n = 0;
+      if (HA_BPERSIST_ITEM_WAIT && s_done_below + 1 == tk.step) {
+        const uint2 d = bdep[tk.step - 1];
+        dep_begin = d.x;
+        dep_task = d.y;
+        dep_n = btasks[tk.step - 1];
+      }
       for_task_items(tk.begin, tk.end, &s_next, [&](uint32_t k) {
-        batched_free_one(k, free_ids, req_ptr, bad, idsum, nfree);
+        const uint32_t r = free_ids[k];
+        if (r >= dep_begin) {
+          const uint32_t t = (r - dep_begin) / items;
+          if (t < dep_n && !ld_acquire_u32(&tdone[dep_task + t])) {
+            const uint64_t limit = now_ns() + 2000000000ull;
+            while (!ld_acquire_u32(&tdone[dep_task + t])) {
+              if (now_ns() > limit) {
+                late++;
+                break;
+              }
+              __nanosleep(64);
+            }
+          }
+        }
+        batched_free_req(r, req_ptr, bad, idsum, nfree);
       });
     } else {
       for_task_items(tk.begin, tk.end, &s_next, [&](uint32_t r) {
@@ -625,7 +671,8 @@ __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uin
       });
       __syncthreads();
       if (threadIdx.x == 0) {
-        __threadfence();  // this block's req_ptr and payload writes before the count
+        __threadfence();  // this block's req_ptr and payload writes before the flags
+        st_relaxed_u32(&tdone[t], 1u);
         atomicAdd(&ctl[1 + tk.step], 1u);
       }
     }
@@ -642,16 +689,19 @@ __global__ void ha_bpersist_k(const BatchTask *tasks, uint32_t ntasks, const uin
 // loops that must not call cudaMalloc/cudaFree because those calls
 // synchronise the device and stall every other stream.  For them the
 // persistent form below keeps its scratch -- the task table, the per-batch
-// task counts, and the queue and completion counters -- in one fixed array
-// in device memory instead.  Every GPU that loads this library holds the
-// array (about 1 MiB) until the process exits.
+// task counts and first tasks, the queue and completion counters, and the
+// per-task done flags -- in one fixed array in device memory instead.  Every
+// GPU that loads this library holds the array (about 1.3 MiB) until the
+// process exits.
 
 constexpr uint32_t kNoAllocMaxTasks = 65536;
 constexpr uint32_t kNoAllocMaxBatches = 1024;
 constexpr size_t kNaTasksOff = 0;
 constexpr size_t kNaBtasksOff = kNaTasksOff + sizeof(BatchTask) * kNoAllocMaxTasks;
 constexpr size_t kNaCtlOff = kNaBtasksOff + 4 * 1280;
-constexpr size_t kNoAllocScratchBytes = kNaCtlOff + 4 * 1280;
+constexpr size_t kNaBdepOff = kNaCtlOff + 4 * 1280;
+constexpr size_t kNaDoneOff = kNaBdepOff + sizeof(uint2) * 1280;
+constexpr size_t kNoAllocScratchBytes = kNaDoneOff + 4 * kNoAllocMaxTasks;
 static_assert(kNoAllocMaxBatches + 2 <= 1280, "scratch regions hold nbatch + 2 words");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -665,8 +715,9 @@ struct NoAllocOffsets {
 };
 
 // Builds the task table of ha_batched_prepare_c (the same order: each step's
-// allocation chunks, then its free chunks) in the scratch array and
-// clears the queue and completion counters.  The host has checked that the
+// allocation chunks, then its free chunks) and the per-batch first request
+// and first task in the scratch array, and clears the queue and completion
+// counters (the host clears the done flags).  The host has checked that the
 // offsets never decrease and that the table has at most kNoAllocMaxTasks
 // entries; indices are 64-bit and the writes stop at the limit regardless.
 __global__ void ha_noalloc_tasks_k(unsigned char *scratch, uint32_t nbatch, uint32_t items,
@@ -675,11 +726,13 @@ __global__ void ha_noalloc_tasks_k(unsigned char *scratch, uint32_t nbatch, uint
   BatchTask *tasks = reinterpret_cast<BatchTask *>(scratch + kNaTasksOff);
   uint32_t *btasks = reinterpret_cast<uint32_t *>(scratch + kNaBtasksOff);
   unsigned int *ctl = reinterpret_cast<unsigned int *>(scratch + kNaCtlOff);
+  uint2 *bdep = reinterpret_cast<uint2 *>(scratch + kNaBdepOff);
   uint32_t n = 0;
   for (uint32_t st = 0; st <= nbatch; st++) {
     ctl[1 + st] = 0;
     if (st < nbatch) {
       btasks[st] = 0;
+      bdep[st] = make_uint2(off.batch_start[st], n);
       const uint64_t b1 = off.batch_start[st + 1];
       for (uint64_t r = off.batch_start[st]; r < b1 && n < kNoAllocMaxTasks; r += items) {
         tasks[n++] = {(uint32_t)r, (uint32_t)(r + items < b1 ? r + items : b1), st, 0u};
@@ -1225,8 +1278,10 @@ struct Batched {
   BatchTask *tasks;
   uint32_t ntasks;
   uint32_t *btasks;  // allocation tasks per batch
-  unsigned int *ctl; // next task, then finished allocation tasks per batch
-  uint32_t grid, block;
+  uint2 *bdep;       // first request and first task index per batch
+  unsigned int *ctl; // next task, finished allocation tasks per batch, then a
+                     // done flag per task
+  uint32_t grid, block, items;
   cudaGraphExec_t exec;
   bool graph;
 };
@@ -1234,10 +1289,12 @@ struct Batched {
 void enqueue_persistent(const Batched *b, cudaStream_t s) {
   unsigned long long *acc = reinterpret_cast<unsigned long long *>(b->plan.acc);
   cudaMemsetAsync(acc, 0, 8 * sizeof(uint64_t), s);
-  cudaMemsetAsync(b->ctl, 0, (b->plan.nbatch + 1) * sizeof(unsigned int), s);
+  cudaMemsetAsync(b->ctl, 0, ((size_t)b->plan.nbatch + 1 + b->ntasks) * sizeof(unsigned int),
+                  s);
   ha_bpersist_k<<<b->grid, b->block, 0, s>>>(
-      b->tasks, b->ntasks, b->btasks, b->plan.req_size,
-      reinterpret_cast<unsigned long long *>(b->plan.req_ptr), b->plan.free_ids, b->ctl, acc);
+      b->tasks, b->ntasks, b->btasks, b->bdep, b->items, b->plan.req_size,
+      reinterpret_cast<unsigned long long *>(b->plan.req_ptr), b->plan.free_ids, b->ctl,
+      b->ctl + b->plan.nbatch + 1, acc);
 }
 
 void release_batched(Batched *b) {
@@ -1245,6 +1302,7 @@ void release_batched(Batched *b) {
   if (b->graph) cudaGraphExecDestroy(b->exec);
   cudaFree(b->tasks);
   cudaFree(b->btasks);
+  cudaFree(b->bdep);
   cudaFree(b->ctl);
   delete b;
 }
@@ -1266,9 +1324,11 @@ extern "C" int ha_batched_prepare_c(const ha_batch_plan_t *plan, uint32_t block,
   // (and has most likely finished), so blocks seldom idle at a step.
   std::vector<BatchTask> tasks;
   std::vector<uint32_t> btasks(plan->nbatch + 1, 0);
+  std::vector<uint2> bdep(plan->nbatch + 1);
   tasks.reserve((size_t)ntasks);
   for (uint32_t st = 0; st <= plan->nbatch; st++) {
     if (st < plan->nbatch) {
+      bdep[st] = make_uint2(plan->h_batch_start[st], (uint32_t)tasks.size());
       const uint64_t b1 = plan->h_batch_start[st + 1];
       for (uint64_t r = plan->h_batch_start[st]; r < b1; r += task_items) {
         tasks.push_back({(uint32_t)r, (uint32_t)(r + task_items < b1 ? r + task_items : b1), st,
@@ -1292,15 +1352,20 @@ extern "C" int ha_batched_prepare_c(const ha_batch_plan_t *plan, uint32_t block,
   b->plan.h_free_start = nullptr;
   b->ntasks = (uint32_t)tasks.size();
   b->block = block;
+  b->items = task_items;
   b->grid = (uint32_t)nsm * (ctas_per_sm && ctas_per_sm < (uint32_t)fit ? ctas_per_sm : fit);
   if (cudaMalloc(&b->tasks, sizeof(BatchTask) * (tasks.empty() ? 1 : tasks.size())) !=
           cudaSuccess ||
       cudaMalloc(&b->btasks, sizeof(uint32_t) * btasks.size()) != cudaSuccess ||
-      cudaMalloc(&b->ctl, (plan->nbatch + 1) * sizeof(unsigned int)) != cudaSuccess ||
+      cudaMalloc(&b->bdep, sizeof(uint2) * bdep.size()) != cudaSuccess ||
+      cudaMalloc(&b->ctl, ((size_t)plan->nbatch + 1 + tasks.size()) * sizeof(unsigned int)) !=
+          cudaSuccess ||
       cudaMemcpy(b->tasks, tasks.data(), sizeof(BatchTask) * tasks.size(),
                  cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(b->btasks, btasks.data(), sizeof(uint32_t) * btasks.size(),
-                 cudaMemcpyHostToDevice) != cudaSuccess) {
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->bdep, bdep.data(), sizeof(uint2) * bdep.size(), cudaMemcpyHostToDevice) !=
+          cudaSuccess) {
     cudaGetLastError();
     release_batched(b);
     return HA_ECUDA;
@@ -1413,13 +1478,17 @@ extern "C" int ha_batched_run_noalloc_c(const ha_batch_plan_t *plan, uint32_t bl
       (uint32_t)nsm * (ctas_per_sm && ctas_per_sm < (uint32_t)fit ? ctas_per_sm : fit);
   cudaStream_t s = as_stream(stream);
   unsigned long long *acc = reinterpret_cast<unsigned long long *>(plan->acc);
-  if (cudaMemsetAsync(acc, 0, 8 * sizeof(uint64_t), s) != cudaSuccess) return HA_ECUDA;
+  if (cudaMemsetAsync(acc, 0, 8 * sizeof(uint64_t), s) != cudaSuccess ||
+      cudaMemsetAsync(scratch + kNaDoneOff, 0, ntasks * sizeof(unsigned int), s) != cudaSuccess)
+    return HA_ECUDA;
   ha_noalloc_tasks_k<<<1, 1, 0, s>>>(scratch, plan->nbatch, task_items, off);
   ha_bpersist_k<<<grid, block, 0, s>>>(
       reinterpret_cast<const BatchTask *>(scratch + kNaTasksOff), (uint32_t)ntasks,
-      reinterpret_cast<const uint32_t *>(scratch + kNaBtasksOff), plan->req_size,
+      reinterpret_cast<const uint32_t *>(scratch + kNaBtasksOff),
+      reinterpret_cast<const uint2 *>(scratch + kNaBdepOff), task_items, plan->req_size,
       reinterpret_cast<unsigned long long *>(plan->req_ptr), plan->free_ids,
-      reinterpret_cast<unsigned int *>(scratch + kNaCtlOff), acc);
+      reinterpret_cast<unsigned int *>(scratch + kNaCtlOff),
+      reinterpret_cast<unsigned int *>(scratch + kNaDoneOff), acc);
   return launch_status();
 }
 

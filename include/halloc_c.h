@@ -433,7 +433,7 @@ int ha_batched_release_c(void *handle);
    loop that must not call cudaMalloc/cudaFree because they synchronise the
    device.  It allocates nothing: the task table and counters live in one
    fixed array of device memory that every GPU loading this library holds
-   until exit (about 1 MiB).  Limits: at most 65,536 tasks (ceil of each
+   until exit (about 1.3 MiB).  Limits: at most 65,536 tasks (ceil of each
    step's frees and of each batch's requests over task_items, summed) and
    1,024 batches, else HA_ERANGE; offsets that decrease or run past nreq
    give HA_EINVAL, checked before anything is launched.  The step offsets
