@@ -672,6 +672,62 @@ __device__ __noinline__ void hand_back(uint32_t hs, uint32_t sb) {
 // by occupancy) and searches again, so NULL still means what it means with
 // one head.  A lone thread never waits for a lock, so it never opens a set
 // and gets exactly the reference's addresses.
+// Opens one more surge level for size sid now, keeping set 0's head slab:
+// the SMs of the new sets find no head of their own and take one through
+// replace_head.  Under set 0's head lock, skipped while another warp holds
+// it (a head change under way makes its own decision); the same headroom
+// gate as at a head change.
+__device__ __forceinline__ void surge_open(uint32_t sid) {
+  uint32_t *hlock = &g_st.head_lock[sid * kTicketStride];
+  if (ld_relaxed(hlock) != 0 || !try_lock(hlock)) return;
+  HA_PSTAT(kPsOpenLocked, 1);
+  uint32_t *head = &g_st.head[sid];
+  const uint32_t w = ld_relaxed(head);
+  const uint32_t level = head_level(w);
+  const uint32_t nfree = ld_relaxed(&g_st.n_free);
+  const uint32_t committed = ld_relaxed(&g_st.committed);
+  if (head_slab(w) != kNone && level < kMaxLevel &&
+      (uint64_t)kSurgeFreeOpen * nfree >= committed) {
+    st_release(head, head_word(head_slab(w), level + 1));
+    red_add(&g_st.n_surge_changes, 1);
+  }
+  unlock(hlock);
+}
+
+// Counts k long-probe lanes of size sid into its probe-storm window.  In a
+// 1 M-thread 16-B x4 phase workload four warps in ten probe long without any
+// storm, so the counting is kept light: one calling warp in 8 (by the SM
+// clock) counts, for 8, with a reduction, and one counting warp in 64 reads
+// the count.  Once the window is full (kProbeStormUp) that warp takes it
+// with an exchange and judges it: a level opens when the size gave out
+// fewer than kProbeStormTickets tickets per long probe since the window
+// began; either way a new window begins.  Only set 0's ticket counter is
+// read: with 2^level sets open it serves that fraction of the SMs, so its
+// count is scaled up by 2^level.  This function must stay a leaf (surge_open
+// is inlined): with a call to a non-inlined function here, a call that never
+// ran, that workload lost a third of its rate.
+__device__ __noinline__ void probe_storm(uint32_t sid, uint32_t k) {
+  const uint32_t c = (uint32_t)clock();
+  if ((c & 7u) != 0) return;
+  uint32_t *line = &g_st.storm[sid * kTicketStride];
+  red_add(line + 2, 8u * k);
+  if ((c & 0x1f8u) != 0 || ld_relaxed(line + 2) < kProbeStormUp) return;
+  const uint32_t got = atomicExch(line + 2, 0u);
+  if (got < kProbeStormUp) {
+    // another warp judged the window just now: give these counts back
+    if (got) red_add(line + 2, got);
+    return;
+  }
+  const uint32_t tnow = ld_relaxed(&g_st.ticket[sid * kTicketStride]);
+  const uint32_t level = head_level(ld_relaxed(&g_st.head[sid]));
+  const bool storm = ((uint64_t)(tnow - ld_relaxed(line + 3)) << level) <
+                     (uint64_t)kProbeStormTickets * got;
+  st_relaxed(line + 3, tnow);
+  HA_PSTAT(kPsJudge, 1);
+  if (storm) HA_PSTAT(kPsStorm, 1);
+  if (storm) surge_open(sid);
+}
+
 __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
   const uint32_t sid = hs % kNSizes, set = hs / kNSizes;
   const bool surge_set = c_cfg.surge && set != 0;
@@ -855,13 +911,20 @@ __device__ __forceinline__ uint32_t next_probe(uint32_t first, uint32_t round, u
 // call -- so addresses, try numbers and give-ups are identical.  Under
 // concurrency a stale word only costs one more try.  Four positions: eight
 // load more than they save once many warps probe a nearly full head (those
-// loads queue on the same few sectors as the atomics).
+// loads queue on the same few sectors as the atomics).  `note` gets
+// kProbeCalm when the call gives up at the end of a round with the count of
+// its last look-ahead below the busy threshold, and kProbeLong when it took
+// kLongProbeRounds look-ahead rounds or more in a slab under half that
+// threshold.
 constexpr uint32_t kLookahead = 4;
+constexpr uint32_t kProbeCalm = 1, kProbeLong = 2;
 __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t mn, uint64_t mh,
                                            uint32_t first, uint32_t block, uint32_t &pos,
-                                           uint32_t &round) {
+                                           uint32_t &round, uint32_t &note) {
   uint32_t *bits = bits_of(sb);
-  for (;;) {
+  note = 0;
+  for (uint32_t nr = 1;; nr++) {
+    HA_PSTAT(kPsRound, 1);
     uint32_t pp[kLookahead], ww[kLookahead];
     pp[0] = pos;
 #pragma unroll
@@ -870,11 +933,13 @@ __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t
 #pragma unroll
     for (uint32_t i = 0; i < kLookahead; i++) ww[i] = ld_meta(&bits[pp[i] >> 5]);
     const uint32_t count = used_of(sb);
+    if (nr >= kLongProbeRounds && 2 * count < c.busy) note |= kProbeLong;
 #pragma unroll
     for (uint32_t i = 0; i < kLookahead; i++) {
       const uint32_t r = round + i;  // try number of position pp[i]
       const uint32_t mask = block << (pp[i] & 31);
       if (!(ww[i] & mask)) {
+        HA_PSTAT(kPsReserve, 1);
         const uint32_t old = atom_or_meta(&bits[pp[i] >> 5], mask);
         if (!(old & mask)) {
           pos = pp[i];
@@ -892,6 +957,7 @@ __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t
       if ((r + 1) % kTriesPerRound >= kTriesPerRound - 1) {
         pos = pp[i];
         round = r + 1;
+        if (count < c.busy) note |= kProbeCalm;
         return false;
       }
     }
@@ -954,6 +1020,7 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
   const uint32_t first = first_probe(sid, ticket, c.ncib, mn, c.nchunks);
   const uint32_t block = (1u << c.ncib) - 1u;
   bool want = flags & kWant, need_head = flags & kNeedHead, mid = flags & kMidRound;
+  bool long_probe = false;
   uint32_t rounds = 0;
   for (;;) {
     // -- new head slabs -------------------------------------------------------
@@ -962,7 +1029,10 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
       const uint32_t lead = __ffs(nmask) - 1;
       const uint32_t lhs = __shfl_sync(warp, hs, lead);
       uint32_t nsb = 0;
-      if (me == lead) nsb = replace_head(hs);
+      if (me == lead) {
+        HA_PSTAT(kPsHead, 1);
+        nsb = replace_head(hs);
+      }
       nsb = __shfl_sync(warp, nsb, lead);
       if (need_head && hs == lhs) {
         if (nsb == kRedirect) {
@@ -990,8 +1060,18 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
         need_head = true;
       } else {
         if (!mid) pos = first;  // a new probe call starts at the first position
-        reserved = probe_from(sb, c, mn, mh, first, block, pos, round);
-        if (!reserved) need_head = true;
+        uint32_t note;
+        reserved = probe_from(sb, c, mn, mh, first, block, pos, round, note);
+        long_probe |= (note & kProbeLong) != 0;
+        // A round that ended in a slab below the busy threshold: the
+        // reference asks for a new head here, and its re-check under the
+        // head lock keeps a head that is not busy and re-reads the head
+        // (src/slab.cuh:384-390,428-431).  The count is known from the
+        // round's last look-ahead, so re-read the head without the lock and
+        // go on probing while it is still this slab; under a probing storm
+        // that spares the head lock tens of thousands of re-checks.
+        if (!reserved && !((note & kProbeCalm) && head_slab(ld_relaxed(&g_st.head[hs])) == sb))
+          need_head = true;
       }
       mid = false;
       const uint32_t rmask = __ballot_sync(want_mask, reserved);
@@ -1008,6 +1088,14 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
     }
   }
   if (!p) red_add(&g_st.n_null, 1);
+  if (HA_PROBE_STORM && c_cfg.surge) {
+    // one count per size group of the warp's lanes that probed long
+    const uint32_t lmask = __ballot_sync(warp, long_probe);
+    if (long_probe) {
+      const uint32_t grp = __match_any_sync(lmask, sid);
+      if (me == (uint32_t)(__ffs(grp) - 1)) probe_storm(sid, __popc(grp));
+    }
+  }
   return p;
 }
 
@@ -1058,6 +1146,7 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
   const uint64_t mn = mod_magic(mm.x, mm.y);
   const uint32_t first = first_probe(sid, ticket, ncib, mn, nchunks);
   const uint32_t block = (1u << ncib) - 1u;
+  HA_PSTAT(kPsAlloc, 1);
 
   uint32_t pos = first, round = 0, flags = kWant;
   bool reserved = false;
@@ -1071,6 +1160,7 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
     if (!(old & mask)) {
       reserved = true;
     } else {
+      HA_PSTAT(kPsFirstMiss, 1);
       if (~old & mask) red_and_meta(w, ~mask | (old & mask));
       // try 0 failed: no count check at an even try; move to try 1
       const uint32_t hstep = __ldg(&g_cls[sid].hash_step);
@@ -1093,6 +1183,7 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
   }
   if (__any_sync(warp, flags != 0)) {
     HA_STAMP(kStSlowIn, flags);
+    if (flags != 0) HA_PSTAT(kPsSlow, 1);
     p = malloc_slow(warp, hs, nbytes, ticket, sb, pos, round, flags, p);
     HA_STAMP(kStSlowOut, (uint32_t)(uintptr_t)p);
   }

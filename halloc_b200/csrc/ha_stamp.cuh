@@ -55,4 +55,37 @@ __device__ __forceinline__ void stamp(uint32_t point, uint32_t dep) {
 #define HA_STAMP(point, dep) ((void)0)
 #endif
 
+// ---------------------------------------------------------------------------
+// probe counters (instrumented builds only: -DHA_PROBE_STATS)
+// ---------------------------------------------------------------------------
+// Per-lane event counts of hamalloc's probing, summed over every launch until
+// read (ha_probe_stats_c).  Each event is one fire-and-forget reduction into
+// one of 32 copies chosen by SM, 128 B apart, so the counting adds no
+// latency to the allocator's chain and no hot word.  Normal builds compile
+// HA_PSTAT to nothing.
+enum ProbeStat : uint32_t {
+  kPsAlloc = 0,    // lanes entering the small-block allocation
+  kPsFirstMiss,    // lanes whose first probe found its chunks taken
+  kPsSlow,         // lanes continuing in the slow path
+  kPsRound,        // look-ahead rounds (4 bit words and the count loaded)
+  kPsReserve,      // reservation atomics issued by the look-ahead
+  kPsHead,         // head replacements asked for (one per warp and head slot)
+  kPsJudge,        // probe-storm windows judged
+  kPsStorm,        // of those, judged a storm
+  kPsOpenLocked,   // surge_open calls that took set 0's head lock
+  kPsCount
+};
+constexpr uint32_t kPsCopies = 32, kPsStride = 16;
+#ifdef HA_PROBE_STATS
+extern __device__ unsigned long long g_pstats[kPsCopies * kPsStride];
+__device__ __forceinline__ void pstat(uint32_t i, uint32_t v) {
+  uint32_t smid;
+  asm("mov.u32 %0, %%smid;" : "=r"(smid));
+  atomicAdd(&g_pstats[(smid % kPsCopies) * kPsStride + i], (unsigned long long)v);
+}
+#define HA_PSTAT(i, v) ::ha::pstat(i, v)
+#else
+#define HA_PSTAT(i, v) ((void)0)
+#endif
+
 }  // namespace ha

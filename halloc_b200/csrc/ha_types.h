@@ -75,6 +75,18 @@ constexpr uint32_t kSurgeQueueMin = 128;
 #ifndef HA_SURGE_FREE_CLOSE
 #define HA_SURGE_FREE_CLOSE 8
 #endif
+// third trigger, probing storms: lanes whose probe call needed
+// kLongProbeRounds or more look-ahead rounds in a slab under half its busy
+// threshold -- a head far from full whose first positions keep meeting taken
+// chunks.  kProbeStormUp of them while the size's set-0 counter gave out
+// fewer than kProbeStormTickets tickets each open a level at once (the head
+// may never fill, so no head change would come to decide it).
+#ifndef HA_PROBE_STORM
+#define HA_PROBE_STORM 1  // 0 builds without the third trigger
+#endif
+constexpr uint32_t kLongProbeRounds = 2;
+constexpr uint32_t kProbeStormUp = 2048;
+constexpr uint32_t kProbeStormTickets = 16;
 constexpr uint32_t kSurgeFreeOpen = HA_SURGE_FREE_OPEN;
 constexpr uint32_t kSurgeFreeClose = HA_SURGE_FREE_CLOSE;
 constexpr uint32_t kSurgeTicketsUp = HA_SURGE_TICKETS_UP;
@@ -136,8 +148,10 @@ struct State {
   // the last head search for (head, size) hs found nothing at that epoch
   alignas(128) uint32_t set_epoch;
   uint32_t no_slab[kMaxHeads * kNSizes];
-  // warps that queued for a size's head lock since the last change of its
-  // set-0 head, capped near kSurgeUp (one 128-B line per size)
+  // per size, one 128-B line: [0] warps that queued for the head lock since
+  // the last change of its set-0 head, capped near kSurgeUp; [1] set 0's
+  // ticket at that change; [2] long-probe lanes in the current probe-storm
+  // window; [3] set 0's ticket when that window began
   alignas(128) uint32_t storm[kNSizes * kTicketStride];
   alignas(128) uint32_t ctr[kMaxSlabs * kCtrStride];
   Desc desc[kMaxSlabs];

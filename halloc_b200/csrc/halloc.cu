@@ -42,6 +42,9 @@ __device__ unsigned long long g_max_alloc;
 __device__ uint2 g_trim_chunks[kMaxSlabs];
 __device__ uint32_t g_trim_out[kMaxSlabs];
 __device__ uint32_t g_trim_n, g_trim_slabs;
+#ifdef HA_PROBE_STATS
+__device__ unsigned long long g_pstats[kPsCopies * kPsStride];
+#endif
 }  // namespace ha
 
 // ---------------------------------------------------------------------------
@@ -967,6 +970,27 @@ extern "C" int ha_set_hash_scale_c(uint32_t percent) {
   g_hash_scale_pct = percent;
   return HA_OK;
 }
+
+#ifdef HA_PROBE_STATS
+// Instrumented builds only: the probe counters (ha_stamp.cuh ProbeStat order)
+// summed over their copies into out[0 .. kPsCount - 1]; reset != 0 zeroes
+// them.  Waits for the device.
+extern "C" int ha_probe_stats_c(unsigned long long *out, int reset) {
+  if (!out) return HA_EINVAL;
+  unsigned long long h[ha::kPsCopies * ha::kPsStride];
+  HA_CK(cudaDeviceSynchronize());
+  HA_CK(cudaMemcpyFromSymbol(h, ha::g_pstats, sizeof(h)));
+  for (uint32_t i = 0; i < ha::kPsCount; i++) {
+    out[i] = 0;
+    for (uint32_t c = 0; c < ha::kPsCopies; c++) out[i] += h[c * ha::kPsStride + i];
+  }
+  if (reset) {
+    memset(h, 0, sizeof(h));
+    HA_CK(cudaMemcpyToSymbol(ha::g_pstats, h, sizeof(h)));
+  }
+  return HA_OK;
+}
+#endif
 
 extern "C" int ha_debug_set_head_lock_c(uint32_t size_id, uint32_t held) {
   if (size_id >= ha::kNSizes || held > 1) return HA_EINVAL;
