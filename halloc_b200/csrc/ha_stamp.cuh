@@ -76,7 +76,10 @@ enum ProbeStat : uint32_t {
   kPsCount
 };
 constexpr uint32_t kPsCopies = 32, kPsStride = 16;
-#ifdef HA_PROBE_STATS
+#ifndef HA_PROBE_STATS
+#define HA_PROBE_STATS 0
+#endif
+#if HA_PROBE_STATS
 extern __device__ unsigned long long g_pstats[kPsCopies * kPsStride];
 __device__ __forceinline__ void pstat(uint32_t i, uint32_t v) {
   uint32_t smid;

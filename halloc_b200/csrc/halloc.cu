@@ -42,7 +42,7 @@ __device__ unsigned long long g_max_alloc;
 __device__ uint2 g_trim_chunks[kMaxSlabs];
 __device__ uint32_t g_trim_out[kMaxSlabs];
 __device__ uint32_t g_trim_n, g_trim_slabs;
-#ifdef HA_PROBE_STATS
+#if HA_PROBE_STATS
 __device__ unsigned long long g_pstats[kPsCopies * kPsStride];
 #endif
 }  // namespace ha
@@ -971,7 +971,7 @@ extern "C" int ha_set_hash_scale_c(uint32_t percent) {
   return HA_OK;
 }
 
-#ifdef HA_PROBE_STATS
+#if HA_PROBE_STATS
 // Instrumented builds only: the probe counters (ha_stamp.cuh ProbeStat order)
 // summed over their copies into out[0 .. kPsCount - 1]; reset != 0 zeroes
 // them.  Waits for the device.

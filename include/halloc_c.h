@@ -167,14 +167,18 @@ int ha_set_heads_c(uint32_t nheads);
    next init on this process).  When thousands of warps queue for one size's
    head replacement during one head's life (2,048 queued warps: a grid of
    1,024 warps can never get there), or when a long queue forms at a head
-   that serves only a few allocations per queued warp (under 96), the size
-   gets 2, then 4, then 8 head slabs, each serving the SMs whose id modulo
-   the set count names it -- while a quarter of the pool's slabs is free.
+   that serves only a few allocations per queued warp (under 96), or when
+   a head under half its busy threshold keeps missing first probes (2,048
+   allocations needing two or more look-ahead rounds within 16 tickets
+   each), the size gets 2, then 4, then 8 head slabs, each serving the SMs
+   whose id modulo the set count names it -- while a quarter of the pool's
+   slabs is free.
    The sets close again one level per calm head change (or while under an
    eighth of the pool is free), and all of them at once when a size runs
    short of slabs, so a NULL still means that no slab is left for the size.
-   A thread alone, or any grid that never queues that many warps, keeps the
-   reference policy's single head and addresses.  0 turns them off (the
+   A thread alone, or any grid that neither queues that many warps nor
+   probes that long, keeps the reference policy's single head and
+   addresses.  0 turns them off (the
    reference policy under every load), 1 on, -1 back to the environment's
    choice; HALLOC_SURGE=0|1 in the environment does the same for programs
    that only use halloc.h.  Ignored
