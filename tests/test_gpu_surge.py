@@ -8,8 +8,10 @@ blocks imply, every slab back in the free set or a head after the last
 free); the plain 32,768-thread workload never opens one; with surge sets off
 a storm keeps the single head; and a storm that exhausts the pool gets as
 many blocks as the single-head policy does (NULL still means no slab is
-left).  The serial-trace parity tests run with surge sets on (the default)
-and show that a lone thread never opens one.
+left); and a probing storm in heads that never fill (32,768 threads each
+holding one 256-B block) opens more levels than the queue alone would.  The
+serial-trace parity tests run with surge sets on (the default) and show that
+a lone thread never opens one.
 """
 import numpy as np
 import pytest
@@ -127,3 +129,42 @@ def test_exhaustion_under_a_storm_gets_what_one_head_gets(torch_cuda, surge_defa
     # busy slabs up to half way to full; surge heads are filed by occupancy
     # when their sets close, so the pool ends about as full
     assert many >= 0.97 * one, (many, one)
+
+
+def _phase_ref_256_private(torch, H, surge: bool):
+    """halloc's phase experiment, 256 B x1, 32,768 threads, private (-i32),
+    four warm-up tries then 16: returns (size-8 surge level, counts equal to
+    the replay's, status, used chunks after the final free)."""
+    from halloc_b200.workloads import group_seeds
+    from oracle.phase import PhaseRefReplay
+    from tests.test_gpu_phase import ref_buffers
+    n, nallocs, niters = 32768, 1, 32
+    probs = H.phase_ref_probabilities(0.95, 0.05, 0.91)
+    seeds = group_seeds(n, 32, 0x5EED)
+    H.set_surge(surge)
+    with allocator(memory=512 << 20) as H:
+        states, slots, ctrs, acc = ref_buffers(torch, seeds, n, nallocs)
+        H.phase_ref_run(n, nallocs, 4, niters, probs, 256, 256, states, slots, ctrs, acc)
+        states.copy_(torch.tensor(seeds.view(np.int32), device="cuda"))
+        acc.zero_()
+        got = H.phase_ref_run(n, nallocs, 16, niters, probs, 256, 256, states, slots, ctrs, acc)
+        r = PhaseRefReplay(seeds, nallocs, probs, 256, 256, niters=niters)
+        for t in range(16):
+            r.step(t)
+        r.rest()
+        same = got["failed"] == 0 and got["mallocs"] == r.mallocs and got["frees"] == r.frees
+        st = assert_free_count(H)
+        return st["surge_level"][8], same, H.status(), st["used_chunks"]
+
+
+def test_probing_storm_opens_levels(torch_cuda, surge_default):
+    """32,768 threads each holding one 256-B block: the heads never fill, so
+    the queue at head changes opens at most one level, while first probes in
+    them keep missing; the probing-storm trigger opens more.  Counts equal
+    the replay's and every block is back after the final free."""
+    torch = torch_cuda
+    level, same, status, used = _phase_ref_256_private(torch, surge_default, True)
+    assert same and status == 0 and used == 0
+    assert level >= 2, level
+    level_off, same, status, used = _phase_ref_256_private(torch, surge_default, False)
+    assert same and status == 0 and used == 0 and level_off == 0
