@@ -649,29 +649,6 @@ __device__ __noinline__ void hand_back(uint32_t hs, uint32_t sb) {
   }
 }
 
-// Gives head slot hs (= set * kNSizes + size id) a new head slab once the
-// current one has reached the busy threshold: the prefetched ("cached") slab
-// first, then a search; the next slab is prefetched right away.  One lane
-// per warp calls this.  A caller that loses the race for the slot's lock
-// waits (bounded) until the head changes or the lock is released (halloc
-// src/slab.cuh:378-445).
-//
-// The lock covers only the switch of the head.  Filing the old head and
-// prefetching the next slab, which the reference also does under the lock,
-// run after it is released, so other warps can use the new head meanwhile;
-// a single thread still performs the reference's steps in the reference's
-// order.  Two prefetches can then overlap: the loser hands its slab back.
-//
-// Surge sets (c_cfg.surge): when thousands of warps queue for one size's
-// head (a grid far larger than its head's free space), the lock holder of
-// set 0 opens more head sets for the size, each serving the SMs whose id
-// modulo 2^level names it, and closes them again as the queue shrinks.  The
-// level travels in set 0's head word.  A set-k slot answers kRedirect (use
-// set 0) when the set is closed or finds no slab; when set 0 itself finds no
-// slab while surge sets are open, it closes them all (their heads are filed
-// by occupancy) and searches again, so NULL still means what it means with
-// one head.  A lone thread never waits for a lock, so it never opens a set
-// and gets exactly the reference's addresses.
 // Opens one more surge level for size sid now, keeping set 0's head slab:
 // the SMs of the new sets find no head of their own and take one through
 // replace_head.  Under set 0's head lock, skipped while another warp holds
@@ -728,6 +705,30 @@ __device__ __noinline__ void probe_storm(uint32_t sid, uint32_t k) {
   if (storm) surge_open(sid);
 }
 
+// Gives head slot hs (= set * kNSizes + size id) a new head slab once the
+// current one has reached the busy threshold: the prefetched ("cached") slab
+// first, then a search; the next slab is prefetched right away.  One lane
+// per warp calls this.  A caller that loses the race for the slot's lock
+// waits (bounded) until the head changes or the lock is released (halloc
+// src/slab.cuh:378-445).
+//
+// The lock covers only the switch of the head.  Filing the old head and
+// prefetching the next slab, which the reference also does under the lock,
+// run after it is released, so other warps can use the new head meanwhile;
+// a single thread still performs the reference's steps in the reference's
+// order.  Two prefetches can then overlap: the loser hands its slab back.
+//
+// Surge sets (c_cfg.surge): when thousands of warps queue for one size's
+// head (a grid far larger than its head's free space), the lock holder of
+// set 0 opens more head sets for the size, each serving the SMs whose id
+// modulo 2^level names it, and closes them again as the queue shrinks.  The
+// level travels in set 0's head word.  A set-k slot answers kRedirect (use
+// set 0) when the set is closed or finds no slab; when set 0 itself finds no
+// slab while surge sets are open, it closes them all (their heads are filed
+// by occupancy) and searches again, so NULL still means what it means with
+// one head.  A lone thread never waits for a lock, so it never opens a set
+// and gets exactly the reference's addresses.  (Probing storms open levels
+// between head changes: probe_storm above.)
 __device__ __noinline__ uint32_t replace_head(uint32_t hs) {
   const uint32_t sid = hs % kNSizes, set = hs / kNSizes;
   const bool surge_set = c_cfg.surge && set != 0;
