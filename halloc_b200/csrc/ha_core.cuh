@@ -914,17 +914,24 @@ __device__ __forceinline__ uint32_t next_probe(uint32_t first, uint32_t round, u
 // load more than they save once many warps probe a nearly full head (those
 // loads queue on the same few sectors as the atomics).  `note` gets
 // kProbeCalm when the call gives up at the end of a round with the count of
-// its last look-ahead below the busy threshold, and kProbeLong when it took
-// kLongProbeRounds look-ahead rounds or more in a slab under half that
-// threshold.
+// its last look-ahead below the busy threshold, and kProbeLong when the
+// lane's allocation has taken kLongProbeRounds look-ahead rounds or more
+// (`nr` counts them across calls) in a slab under half that threshold.  `held` is a block's worth of the slab's count that the caller
+// already added (its early count, kCredit): the count it reads is taken as
+// that much lower -- as the reference's thread, which has counted nothing
+// yet, reads it -- and the call stops after one look-ahead round with
+// kProbeMore (pos and round then name the next try), so that the early
+// count is used or given back soon.
 constexpr uint32_t kLookahead = 4;
-constexpr uint32_t kProbeCalm = 1, kProbeLong = 2;
+constexpr uint32_t kProbeCalm = 1, kProbeLong = 2, kProbeMore = 4;
 __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t mn, uint64_t mh,
                                            uint32_t first, uint32_t block, uint32_t &pos,
-                                           uint32_t &round, uint32_t &note) {
+                                           uint32_t &round, uint32_t held, uint32_t &nr,
+                                           uint32_t &note) {
   uint32_t *bits = bits_of(sb);
   note = 0;
-  for (uint32_t nr = 1;; nr++) {
+  for (;;) {
+    nr++;
     HA_PSTAT(kPsRound, 1);
     uint32_t pp[kLookahead], ww[kLookahead];
     pp[0] = pos;
@@ -933,7 +940,7 @@ __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t
       pp[i] = next_probe(first, round + i - 1, c.ncib, c.nchunks, mn, c.hash_step, mh);
 #pragma unroll
     for (uint32_t i = 0; i < kLookahead; i++) ww[i] = ld_meta(&bits[pp[i] >> 5]);
-    const uint32_t count = used_of(sb);
+    const uint32_t count = used_of(sb) - held;
     if (nr >= kLongProbeRounds && 2 * count < c.busy) note |= kProbeLong;
 #pragma unroll
     for (uint32_t i = 0; i < kLookahead; i++) {
@@ -964,14 +971,21 @@ __device__ __forceinline__ bool probe_from(uint32_t sb, const Class &c, uint64_t
     }
     pos = next_probe(first, round + kLookahead - 1, c.ncib, c.nchunks, mn, c.hash_step, mh);
     round += kLookahead;
+    if (held) {
+      note |= kProbeMore;
+      return false;
+    }
   }
 }
 
 // Counts the blocks just reserved by the lanes of rmask, one atomic per slab
 // (halloc src/slab.cuh:122-155).  Called by exactly the lanes of rmask.
-// Returns false, after undoing this lane's reservation, when the slab no
-// longer has the caller's chunk size; otherwise *crossed tells whether the
-// count crossed the busy threshold.
+// Returns false, after giving this lane's block back, when the slab no
+// longer has the caller's chunk size: the lane's ncib chunks of count then
+// stay added, and the caller hands them to the slow path as a credit, which
+// takes them back off before its head request (no call here, so hamalloc's
+// frame stays small).  Otherwise *crossed tells whether the count crossed
+// the busy threshold.
 __device__ __forceinline__ bool commit(uint32_t rmask, uint32_t sb, uint32_t ncib,
                                        uint32_t cid, uint32_t busy, uint32_t pos,
                                        uint32_t block, bool &crossed) {
@@ -984,12 +998,7 @@ __device__ __forceinline__ bool commit(uint32_t rmask, uint32_t sb, uint32_t nci
   const bool ok = ((before >> kChunkShift) & kChunkField) == cid;
   const uint32_t n0 = before >> kCntShift;
   crossed = n0 + total >= busy && n0 < busy;
-  const uint32_t cmask = __ballot_sync(rmask, !ok);
-  if (!ok) {
-    // the slab changed chunk size under us: give the block back
-    red_and_meta(&bits_of(sb)[pos >> 5], ~(block << (pos & 31)));
-    count_down(cmask, sb, ncib);
-  }
+  if (!ok) red_and_meta(&bits_of(sb)[pos >> 5], ~(block << (pos & 31)));
   return ok;
 }
 
@@ -1004,6 +1013,8 @@ __device__ __forceinline__ void *publish(uint32_t sb, uint32_t pos, uint32_t enc
 constexpr uint32_t kWant = 1;      // no block yet
 constexpr uint32_t kNeedHead = 2;  // ask for a new head slab
 constexpr uint32_t kMidRound = 4;  // continue the current probe call at pos
+constexpr uint32_t kCredit = 8;    // a block's worth of sb's count is already this lane's
+constexpr uint32_t kCreditCrossed = 16;  // that early count crossed the busy threshold
 
 // The rest of halloc's allocation loop (src/halloc.cu:145-179 with
 // src/slab.cuh:453-535), for the whole warp `warp`: new head slabs for the
@@ -1022,8 +1033,31 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
   const uint32_t block = (1u << c.ncib) - 1u;
   bool want = flags & kWant, need_head = flags & kNeedHead, mid = flags & kMidRound;
   bool long_probe = false;
+  // kCredit: the lane added a block's worth (ncib chunks) of sb's count with
+  // no block to show for it -- malloc_small's early count for a reservation
+  // that failed, or a commit in a slab that changed chunk size.  The first
+  // (one look-ahead round long) probe call may use it: a block reserved in
+  // sb is then already counted.  Otherwise it goes back right after that
+  // call, one atomic per (warp, slab), whose returned value is looked at
+  // only on the way out (a slab that is no longer a head is then filed like
+  // any count-down); or, for a lane that needs a new head first, before its
+  // head request, so that the old head is filed by its true count.
+  uint32_t credit = (flags & kCredit) ? sb : kNone;
+  const bool credit_crossed = flags & kCreditCrossed;
+  uint32_t ret_before = 0, ret_total = 0, ret_sb = kNone;
+  uint32_t lookahead_rounds = 0;  // this lane's, over all its probe calls
   uint32_t rounds = 0;
   for (;;) {
+    if (want && ++rounds > kMaxRounds) {
+      raise_status(HA_ST_LIVELOCK);
+      want = false;
+    }
+    const bool back = credit != kNone && (need_head || !want);
+    const uint32_t cmask = __ballot_sync(warp, back);
+    if (back) {
+      count_down(cmask, credit, c.ncib);
+      credit = kNone;
+    }
     // -- new head slabs -------------------------------------------------------
     uint32_t nmask = __ballot_sync(warp, need_head);
     while (nmask) {
@@ -1049,20 +1083,17 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
       }
       nmask = __ballot_sync(warp, need_head);
     }
-    if (want && ++rounds > kMaxRounds) {
-      raise_status(HA_ST_LIVELOCK);
-      want = false;
-    }
     const uint32_t want_mask = __ballot_sync(warp, want);
     if (!want_mask) break;
     if (want) {
       bool reserved = false;
+      uint32_t note = 0;
       if (sb == kNone) {
         need_head = true;
       } else {
         if (!mid) pos = first;  // a new probe call starts at the first position
-        uint32_t note;
-        reserved = probe_from(sb, c, mn, mh, first, block, pos, round, note);
+        reserved = probe_from(sb, c, mn, mh, first, block, pos, round,
+                              credit != kNone ? c.ncib : 0u, lookahead_rounds, note);
         long_probe |= (note & kProbeLong) != 0;
         // A round that ended in a slab below the busy threshold: the
         // reference asks for a new head here, and its re-check under the
@@ -1071,12 +1102,31 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
         // round's last look-ahead, so re-read the head without the lock and
         // go on probing while it is still this slab; under a probing storm
         // that spares the head lock tens of thousands of re-checks.
-        if (!reserved && !((note & kProbeCalm) && head_slab(ld_relaxed(&g_st.head[hs])) == sb))
+        if (!reserved && !(note & kProbeMore) &&
+            !((note & kProbeCalm) && head_slab(ld_relaxed(&g_st.head[hs])) == sb))
           need_head = true;
       }
-      mid = false;
-      const uint32_t rmask = __ballot_sync(want_mask, reserved);
-      if (reserved) {
+      mid = (note & kProbeMore) != 0;  // one look-ahead round done: go on at pos
+      const bool counted = reserved && credit != kNone;
+      const bool give_back = !reserved && credit != kNone;
+      const uint32_t gmask = __ballot_sync(want_mask, give_back);
+      if (give_back) {
+        const uint32_t grp = __match_any_sync(gmask, credit);
+        const uint32_t total = __reduce_add_sync(grp, c.ncib);
+        if (me == (uint32_t)(__ffs(grp) - 1)) {
+          ret_before = atom_add_meta(ctr_of(credit), 0u - (total << kCntShift));
+          ret_total = total;
+          ret_sb = credit;
+        }
+        credit = kNone;
+      }
+      const uint32_t rmask = __ballot_sync(want_mask, reserved && !counted);
+      if (counted) {
+        if (credit_crossed) need_head = true;
+        p = publish(sb, pos, c.chunk_enc, c.ncib);
+        credit = kNone;
+        want = false;
+      } else if (reserved) {
         bool crossed;
         if (commit(rmask, sb, c.ncib, c.chunk_id, c.busy, pos, block, crossed)) {
           if (crossed) need_head = true;
@@ -1084,10 +1134,12 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
           want = false;
         } else {
           need_head = true;
+          credit = sb;  // the count commit() added goes back at the loop's top
         }
       }
     }
   }
+  if (ret_sb != kNone && !(ret_before & kHeadFlag)) file_after_free(ret_sb, ret_before, ret_total);
   if (!p) red_add(&g_st.n_null, 1);
   if (HA_PROBE_STORM && c_cfg.surge) {
     // one count per size group of the warp's lanes that probed long
@@ -1151,18 +1203,38 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
 
   uint32_t pos = first, round = 0, flags = kWant;
   bool reserved = false;
+  // The reservation's atomic, and for a one-chunk size (c_cfg.spec_mask) the
+  // slab count's as well, one per (warp, slab), in the same round trip: the
+  // count is added before the reservation is known to have succeeded.  Only
+  // while the size has no surge set open: under a storm the counts of
+  // reservations that failed would swell a head's count for a look-ahead
+  // round, and the probing-storm trigger reads that count.
+  const bool spec = sb != kNone && head_level(w) == 0 && ((c_cfg.spec_mask >> sid) & 1u);
+  uint32_t *bw = nullptr;
+  uint32_t mask = 0, old = 0;
+  if (sb != kNone) {
+    mask = block << (pos & 31);
+    bw = &bits_of(sb)[pos >> 5];
+    old = atom_or_meta(bw, mask);
+  }
+  const uint32_t smask = __ballot_sync(warp, spec);
+  uint32_t sgrp = 0, before = 0;
+  if (spec) {
+    sgrp = __match_any_sync(smask, sb);
+    const uint32_t lead = __ffs(sgrp) - 1;
+    if (lane_id() == lead)
+      before = atom_add_meta(ctr_of(sb), (uint32_t)__popc(sgrp) << kCntShift);
+    before = __shfl_sync(sgrp, before, lead);
+  }
   if (sb == kNone) {
     flags |= kNeedHead;
   } else {
-    const uint32_t mask = block << (pos & 31);
-    uint32_t *w = &bits_of(sb)[pos >> 5];
-    const uint32_t old = atom_or_meta(w, mask);
     HA_STAMP(kStMallocProbe, old);
     if (!(old & mask)) {
       reserved = true;
     } else {
       HA_PSTAT(kPsFirstMiss, 1);
-      if (~old & mask) red_and_meta(w, ~mask | (old & mask));
+      if (~old & mask) red_and_meta(bw, ~mask | (old & mask));
       // try 0 failed: no count check at an even try; move to try 1
       const uint32_t hstep = __ldg(&g_cls[sid].hash_step);
       pos = next_probe(first, 0, ncib, nchunks, mn, hstep, mod_magic(mm.z, mm.w));
@@ -1171,15 +1243,37 @@ __device__ __forceinline__ void *malloc_small(uint32_t nbytes) {
     }
   }
   void *p = nullptr;
-  const uint32_t rmask = __ballot_sync(warp, reserved);
-  if (reserved) {
+  if (spec) {
+    // the early count: as commit() below, for the whole group at once.  A
+    // lane whose reservation failed hands its chunk of count to the slow
+    // path as a credit (kCredit), with whether the early count crossed the
+    // busy threshold; so does a lane whose slab changed chunk size under it
+    // (its block goes back here), which asks for a new head at once (no
+    // call here, so hamalloc's frame stays small).
+    HA_STAMP(kStMallocCount, before);
+    const uint32_t n0 = before >> kCntShift, total = __popc(sgrp);
+    const uint32_t busy = __ldg(&g_cls[sid].busy);
+    const bool crossed = n0 + total >= busy && n0 < busy;
+    if (((before >> kChunkShift) & kChunkField) != cid) {
+      if (reserved) red_and_meta(bw, ~mask);
+      reserved = false;
+      flags = kWant | kNeedHead | kCredit;
+    } else if (reserved) {
+      p = publish(sb, pos, enc, 1u);
+      flags = crossed ? kNeedHead : 0;
+    } else {
+      flags |= kCredit | (crossed ? kCreditCrossed : 0u);
+    }
+  }
+  const uint32_t rmask = __ballot_sync(warp, reserved && !spec);
+  if (reserved && !spec) {
     bool crossed;
     if (commit(rmask, sb, ncib, cid, __ldg(&g_cls[sid].busy), pos, block, crossed)) {
       HA_STAMP(kStMallocCount, crossed);
       p = publish(sb, pos, enc, ncib);
       flags = crossed ? kNeedHead : 0;
     } else {
-      flags = kWant | kNeedHead;
+      flags = kWant | kNeedHead | kCredit;
     }
   }
   if (__any_sync(warp, flags != 0)) {

@@ -127,7 +127,18 @@ struct Config {
   uint32_t nheads;        // head slabs per size, a power of two <= kMaxHeads
   uint32_t growth;        // 1: slabs are backed on demand (ha_grow_c)
   uint32_t surge;         // 1: head sets 1.. open under contention (nheads == 1 only)
+  uint32_t spec_mask;     // bit s: size s adds its slab count with the reservation
 };
+
+// Early count: size classes whose blocks are one chunk (16, 24, 256, 384 B)
+// add their slab count in the same round trip as the bit reservation, and a
+// lane whose reservation failed keeps that chunk of count as a credit in the
+// slow path.  Each thread holds at most one such chunk, so a class qualifies
+// when its slab's chunk count plus every thread the device can hold fits in
+// the count field (checked at init).  -DHA_SPEC_COMMIT=0 builds without it.
+#ifndef HA_SPEC_COMMIT
+#define HA_SPEC_COMMIT 1
+#endif
 
 // mutable allocator state (global memory, one instance per device)
 // per-head arrays are indexed [ihead * kNSizes + size]; head 0 is the one

@@ -488,6 +488,13 @@ int init_impl(const ha_opts_c &o) {
     cfg.nheads = heads_for_init();
     cfg.surge = surge_for_init(cfg.nheads);
     cfg.growth = grow.growth ? 1 : 0;
+    if (HA_SPEC_COMMIT) {
+      const uint64_t resident =
+          (uint64_t)prop.multiProcessorCount * (uint64_t)prop.maxThreadsPerMultiProcessor;
+      for (uint32_t s = 0; s < ha::kNSizes; s++)
+        if (cls[s].ncib == 1 && cls[s].nchunks + resident < (1ull << (32 - ha::kCntShift)))
+          cfg.spec_mask |= 1u << s;
+    }
     if (cudaMemset(meta, 0, meta_bytes) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_cls, cls, sizeof(cls)) != cudaSuccess ||
         cudaMemcpyToSymbol(ha::g_mod, mod, sizeof(mod)) != cudaSuccess ||
