@@ -76,3 +76,14 @@ def test_pyfast_binding_checks_arguments():
     # d_out NULL: HA_EINVAL from both bindings
     args = (0, 0, 16, 1, 128, 1, 1, 0, 8, 0, 0)
     assert H._pyfast.throughput_host(*args) == H.load().ha_throughput_host_ex_c(*args) == -1
+
+
+def test_probe_counters_only_in_instrumented_builds():
+    """The probe counters (ha_probe_stats_c) are compiled in only with
+    -DHA_PROBE_STATS: the normal library does not export them, and the
+    probe-counter tool stops before any GPU work, naming the build flag."""
+    from halloc_b200 import probestats
+    assert not hasattr(H.load(), "ha_probe_stats_c")
+    with pytest.raises(SystemExit) as e:
+        probestats.run(1, True)
+    assert "HA_PROBE_STATS" in str(e.value)
