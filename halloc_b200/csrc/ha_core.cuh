@@ -671,11 +671,12 @@ __device__ __forceinline__ void surge_open(uint32_t sid) {
   unlock(hlock);
 }
 
-// Counts k long-probe lanes of size sid into its probe-storm window.  In a
-// 1 M-thread 16-B x4 phase workload four warps in ten probe long without any
-// storm, so the counting is kept light: one calling warp in 8 (by the SM
-// clock) counts, for 8, with a reduction, and one counting warp in 64 reads
-// the count.  Once the window is full (kProbeStormUp) that warp takes it
+// Counts k long-probe lanes of size sid, for 8 (the caller samples one warp
+// in 8 by the SM clock `c`, the same for the whole warp), into its
+// probe-storm window with a reduction: in a 1 M-thread 16-B x4 phase
+// workload four warps in ten probe long without any storm, so the counting
+// is kept light, and one counting warp in 64 (more bits of `c`) reads the
+// count.  Once the window is full (kProbeStormUp) that warp takes it
 // with an exchange and judges it: a level opens when the size gave out
 // fewer than kProbeStormTickets tickets per long probe since the window
 // began; either way a new window begins.  Only set 0's ticket counter is
@@ -683,9 +684,7 @@ __device__ __forceinline__ void surge_open(uint32_t sid) {
 // count is scaled up by 2^level.  This function must stay a leaf (surge_open
 // is inlined): with a call to a non-inlined function here, a call that never
 // ran, that workload lost a third of its rate.
-__device__ __noinline__ void probe_storm(uint32_t sid, uint32_t k) {
-  const uint32_t c = (uint32_t)clock();
-  if ((c & 7u) != 0) return;
+__device__ __noinline__ void probe_storm(uint32_t sid, uint32_t k, uint32_t c) {
   uint32_t *line = &g_st.storm[sid * kTicketStride];
   red_add(line + 2, 8u * k);
   if ((c & 0x1f8u) != 0 || ld_relaxed(line + 2) < kProbeStormUp) return;
@@ -1142,11 +1141,16 @@ __device__ __noinline__ void *malloc_slow(uint32_t warp, uint32_t hs, uint32_t n
   if (ret_sb != kNone && !(ret_before & kHeadFlag)) file_after_free(ret_sb, ret_before, ret_total);
   if (!p) red_add(&g_st.n_null, 1);
   if (HA_PROBE_STORM && c_cfg.surge) {
-    // one count per size group of the warp's lanes that probed long
-    const uint32_t lmask = __ballot_sync(warp, long_probe);
-    if (long_probe) {
-      const uint32_t grp = __match_any_sync(lmask, sid);
-      if (me == (uint32_t)(__ffs(grp) - 1)) probe_storm(sid, __popc(grp));
+    // one warp in 8 (by the SM clock, one lane's reading for the whole warp)
+    // counts, for 8, one count per size group of its lanes that probed long;
+    // the other warps skip the collectives and the call
+    const uint32_t c = __shfl_sync(warp, (uint32_t)clock(), __ffs(warp) - 1);
+    if ((c & 7u) == 0) {
+      const uint32_t lmask = __ballot_sync(warp, long_probe);
+      if (long_probe) {
+        const uint32_t grp = __match_any_sync(lmask, sid);
+        if (me == (uint32_t)(__ffs(grp) - 1)) probe_storm(sid, __popc(grp), c);
+      }
     }
   }
   return p;
